@@ -1,0 +1,179 @@
+/* C-ABI of the B200 SpecAnn engine (libspecann_b200.so).
+ *
+ * Plain pointers and sizes only. Device buffers are allocated by the caller (the Python host uses
+ * torch) and passed as raw device pointers together with a cudaStream_t (as void*). Every entry
+ * point returns an int status (sa_status below); none of them allocates device memory.
+ *
+ * Each declaration names the reference interface it replaces (paths inside the reference
+ * repository Vgueca/SpecAnn).
+ */
+#ifndef SPECANN_B200_H
+#define SPECANN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The Python host maps them onto the reference's exceptions
+ * (models/spectral_annealing.py:70-77 EigensolverBreakdown, utils/failures.py:4-25
+ * NumericalFailure / out-of-memory). */
+typedef enum {
+  SA_OK = 0,
+  SA_ERR_BREAKDOWN = 1,        /* Lanczos breakdown: non-finite or impossible Ritz matrix entry */
+  SA_ERR_NONFINITE = 2,        /* non-finite eigenvalue or eigenvector */
+  SA_ERR_NOT_CONVERGED = 3,    /* stopped at maxiter above tol (the pair is still returned) */
+  SA_ERR_OOM = 4,              /* workspace too small */
+  SA_ERR_INVALID_ARG = 5,
+  SA_ERR_CUDA = 6,             /* a CUDA runtime call failed */
+  SA_ERR_BARRIER_TIMEOUT = 7   /* a bounded grid-barrier wait ran out (kernel returned early) */
+} sa_status;
+
+/* Start vector of an alpha solve (models/spectral_annealing.py:589-612). */
+typedef enum {
+  SA_START_RANDOM = 0,     /* cold start: a seeded standard-normal vector */
+  SA_START_PREV = 1,       /* the previous eigenvector y_last as is (pred_mode "prev") */
+  SA_START_DIAGONAL = 2,   /* utils/predictors.py:6-26, then the residual acceptance test */
+  SA_START_SECANT = 3,     /* utils/predictors.py:29-56, then the residual acceptance test */
+  SA_START_GIVEN = 4       /* the device vector passed in sa_alpha_params.v0 */
+} sa_start_mode;
+
+typedef struct sa_handle sa_handle;
+
+typedef struct {
+  double alpha;          /* normalisation exponent of this solve */
+  double alpha_prev;     /* alpha of y_last (diagonal predictor step) */
+  double rho;            /* shift: S_rho = rho I - N_alpha */
+  double gershgorin;     /* g = max d^(1 - alpha): bound used by the Ritz-matrix guard */
+  double tol;            /* Lanczos residual-estimate tolerance (eigsh_tol) */
+  double pred_tol;       /* predictor acceptance tolerance */
+  double secant_gamma;   /* secant step (1.0 in the reference) */
+  int32_t maxiter;       /* maximum Lanczos matvecs (eigsh_maxiter) */
+  int32_t ncv;           /* Lanczos basis size (<= the handle's ncv_max) */
+  int32_t start_mode;    /* sa_start_mode */
+  int32_t align;         /* 1: sign-align the result with y_last (when a y_last exists) */
+  uint64_t seed;         /* seed of the random start stream */
+  int64_t stream_id;     /* random stream id (alpha index and attempt) */
+  const void* v0;        /* device start vector for SA_START_GIVEN (else NULL) */
+  int32_t round;         /* 1: round x = D^{-1/2} y to packed spins and hash them */
+  int32_t residual_check;/* 1: true residual ||S y - mu y|| with one more SpMV */
+} sa_alpha_params;
+
+typedef struct {
+  int32_t status;        /* sa_status of this solve */
+  int32_t iterations;    /* Lanczos matvecs (the predictor test matvec not counted) */
+  int32_t restarts;      /* thick restarts */
+  int32_t pred_accepted; /* -1 no predictor ran, 0 rejected (restarted from y_last), 1 accepted */
+  double mu;             /* smallest eigenvalue of S_rho (Ritz value) */
+  double lambda1;        /* rho - mu: leading eigenvalue of N_alpha */
+  double residual;       /* ||S y - mu y|| / ||y|| with FP64 accumulation (NaN if not checked) */
+  double res_estimate;   /* Lanczos estimate |b_j s_j| */
+  double pred_residual;  /* ||N y0 - (y0.N y0) y0|| of the predicted start (NaN if none) */
+  double degree_scale;   /* sum_i d_i^alpha (the per-alpha CSV column degree_scale) */
+  double align_dot;      /* y . y_last before the sign alignment (0 without y_last) */
+  uint64_t signature;    /* 64-bit hash of the packed rounded spins */
+  int32_t nonfinite;     /* 1 if the eigenvector had a non-finite entry */
+  int32_t basis_used;    /* basis vectors in use at the end */
+} sa_alpha_record;
+
+typedef struct {
+  int32_t k;                    /* candidates (slots first_slot .. first_slot + k - 1) */
+  int32_t first_slot;           /* first candidate slot (0 for the batched search) */
+  int32_t max_iterations;       /* main-loop passes (max_local_iterations) */
+  double subset_fraction;       /* 0.9 */
+  double final_sweep_fraction;  /* 1.0 */
+  int32_t final_sweep_iters;    /* 25 */
+  int32_t num_rounds;           /* 25 */
+  uint64_t seed;                /* node-selection stream seed */
+} sa_ls_params;
+
+typedef struct {
+  int32_t status;
+  int32_t iterations;           /* main-loop passes used (flip_refinement's max_iters_used) */
+  int32_t final_passes;         /* passes run by the final sweep */
+  int32_t integer_gains;        /* 1: int32 gains (bit-exact); 0: FP64 gains */
+  int64_t total_flips;
+} sa_ls_result;
+
+/* ---- workspace and handle ------------------------------------------------------------------ */
+
+/* Bytes of device workspace for a handle (no reference counterpart: CuPy's memory pool,
+ * models/spectral_annealing.py:493-496, is replaced by one caller-owned buffer). */
+int sa_workspace_size(int64_t n, int64_t nnz, int32_t rowptr64, int32_t precision,
+                      int32_t ncv_max, int32_t max_candidates, size_t* bytes);
+
+/* Create a solver handle over a caller-owned workspace (replaces the per-solve CuPy setup of
+ * SpectralAnnealing.solve, models/spectral_annealing.py:262-288). precision: 32 or 64. */
+int sa_create(sa_handle** out, int64_t n, int64_t nnz, int32_t rowptr64, int32_t precision,
+              int32_t ncv_max, int32_t max_candidates, void* workspace, size_t workspace_bytes,
+              void* stream);
+int sa_destroy(sa_handle* h);
+
+/* Bind the device CSR (rowptr: int32 or int64 per rowptr64; col: int32; val: float or double per
+ * precision; symmetric, zero diagonal) and run the prelude of models/spectral_annealing.py:270-288:
+ * absolute degrees, c = max degree, d = deg / c, log2 d; build the SpMV work list. Reports c,
+ * min/max of d and whether every coupling is an integer (int32 gains in the local search). */
+int sa_set_matrix(sa_handle* h, const void* rowptr, const int32_t* col, const void* val,
+                  double* norm_c, double* d_min, double* d_max, int32_t* integer_couplings);
+
+/* y = rho x - N_alpha x with N_alpha = D^{-1/2} (J/c) D^{-1/2}, D = max(d^alpha, 1e-12): the
+ * fused operator of NAlphaOperator/SRhoOperator (models/spectral_annealing.py:29-53). x, y are
+ * device vectors of the handle's precision. */
+int sa_spmv_scaled(sa_handle* h, double alpha, double rho, const void* x, void* y);
+
+/* One alpha of the sweep (models/spectral_annealing.py:568-669 with utils/eigsh.py:10-17 and
+ * utils/predictors.py): start vector / predictor with its residual test, warm-started
+ * thick-restart Lanczos for the smallest eigenpair of S_rho with the Ritz-matrix guard
+ * (:85-120), sign alignment with y_last and normalisation (:653-663), optional true residual
+ * (:636-647), and the rounding s = sign(x >= 0) of x = D^{-1/2} y (:345) packed into the scratch
+ * candidate with its signature (:557-561). One cooperative launch. */
+int sa_alpha_solve(sa_handle* h, const sa_alpha_params* p, sa_alpha_record* rec);
+
+/* The last solved eigenvector y (unit norm, aligned) as a device pointer valid until the next
+ * sa_alpha_solve or sa_commit_alpha. */
+int sa_result_vector(sa_handle* h, const void** y);
+
+/* Accept the last solve as the new warm start: y_prev <- y_last <- y
+ * (models/spectral_annealing.py:330-342). */
+int sa_commit_alpha(sa_handle* h);
+
+/* Set y_last (and clear y_prev) from a device vector (tests, external warm starts). */
+int sa_set_last_vector(sa_handle* h, const void* y);
+
+/* Rounding only: align a given device eigenvector with y_last (if align), normalise it, form
+ * x = D^{-1/2} y for this alpha and round it into the scratch candidate
+ * (models/spectral_annealing.py:345, :557-561). */
+int sa_round_vector(sa_handle* h, double alpha, const void* y, int32_t align, uint64_t* signature);
+
+/* Candidate store (the dict of models/spectral_annealing.py:362-370): copy the scratch
+ * candidate into slot; compare it with a slot; copy packed words in or out; unpack to int8. */
+int sa_candidate_keep(sa_handle* h, int32_t slot);
+int sa_candidate_equal(sa_handle* h, int32_t slot, int32_t* equal);
+int sa_candidate_set(sa_handle* h, int32_t slot, const uint32_t* packed_device);
+int sa_candidate_get(sa_handle* h, int32_t slot, int32_t refined, uint32_t* packed_device);
+int sa_candidate_unpack(sa_handle* h, int32_t slot, int32_t refined, int8_t* spins_device);
+
+/* Bytes of device workspace for a local search over k candidates. */
+int sa_ls_workspace_size(sa_handle* h, int32_t k, size_t* bytes);
+
+/* Batched local search of candidate slots first_slot..first_slot+k-1 (flip_refinement + gpu_final_sweep,
+ * models/spectral_annealing.py:983-1112) as one persistent kernel with snapshot passes and the
+ * counter-based node selection; also the energies before and after
+ * (models/spectral_annealing.py:693-720, :925-976). Refined spins go to the refined store.
+ * energies_*: host arrays of k doubles (exact integers for integer couplings). */
+int sa_local_search(sa_handle* h, const sa_ls_params* p, void* ls_workspace, size_t ls_bytes,
+                    double* energies_before, double* energies_after, sa_ls_result* result);
+
+/* Energies E = -1/2 s^T J s of candidate slots 0..k-1 (no local search): _batch_energies /
+ * fp32_energies, models/spectral_annealing.py:693-707, :962-976. */
+int sa_energies(sa_handle* h, int32_t k, void* ls_workspace, size_t ls_bytes, double* energies);
+
+/* Version string of the library. */
+const char* sa_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPECANN_B200_H */

@@ -1,0 +1,19 @@
+"""CPU oracle for the SpecAnn alpha-sweep hot path.
+
+TEST INFRASTRUCTURE ONLY. Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg
+(and its ``--impl reference`` arm) may import anything here, and only as the checker or the timed
+CPU baseline. The product (specann_b200) never imports, links or calls this package: it has no CPU
+fallback.
+
+Modules:
+  specann_oracle  NumPy/SciPy restatement of the reference solver (prelude, schedule, operators,
+                  shift, predictors, eigensolve with retry/checks, rounding, signatures, energies,
+                  local search, best-candidate selection).
+  selection       the counter-based node-selection stream shared with the CUDA local search.
+  graphs          seeded Barabasi-Albert / Erdos-Renyi generators used for synthetic inputs.
+  ls_oracle.c     the same local search and energies in plain C (for CPU baselines at large n).
+
+Parity pin: tests/golden/make_golden.py runs the reference's own solver code (the CuPy files of the
+reference, executed on NumPy/SciPy through a stand-in module) and freezes its per-alpha records;
+tests/test_oracle_golden.py checks this oracle against them.
+"""

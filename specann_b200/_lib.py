@@ -1,0 +1,144 @@
+"""ctypes binding of libspecann_b200.so (the C-ABI declared in include/specann_b200.h).
+
+The library is built in-tree by specann_b200/build.py. There is no CPU fallback: when the library is
+missing or no CUDA device is present, every call that would compute raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+from .failures import EigensolverBreakdown, NumericalFailure, SpecAnnOutOfMemory
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libspecann_b200.so"
+GRAPH_LIB_PATH = PKG / "libspecann_graphs.so"
+
+SA_OK = 0
+SA_ERR_BREAKDOWN = 1
+SA_ERR_NONFINITE = 2
+SA_ERR_NOT_CONVERGED = 3
+SA_ERR_OOM = 4
+SA_ERR_INVALID_ARG = 5
+SA_ERR_CUDA = 6
+SA_ERR_BARRIER_TIMEOUT = 7
+
+STATUS_NAMES = {0: "OK", 1: "BREAKDOWN", 2: "NONFINITE", 3: "NOT_CONVERGED", 4: "OOM", 5: "INVALID_ARG",
+                6: "CUDA_ERROR", 7: "BARRIER_TIMEOUT"}
+
+SA_START_RANDOM, SA_START_PREV, SA_START_DIAGONAL, SA_START_SECANT, SA_START_GIVEN = range(5)
+
+
+class AlphaParams(C.Structure):
+    _fields_ = [("alpha", C.c_double), ("alpha_prev", C.c_double), ("rho", C.c_double),
+                ("gershgorin", C.c_double), ("tol", C.c_double), ("pred_tol", C.c_double),
+                ("secant_gamma", C.c_double), ("maxiter", C.c_int32), ("ncv", C.c_int32),
+                ("start_mode", C.c_int32), ("align", C.c_int32), ("seed", C.c_uint64),
+                ("stream_id", C.c_int64), ("v0", C.c_void_p), ("round", C.c_int32),
+                ("residual_check", C.c_int32)]
+
+
+class AlphaRecord(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("restarts", C.c_int32),
+                ("pred_accepted", C.c_int32), ("mu", C.c_double), ("lambda1", C.c_double),
+                ("residual", C.c_double), ("res_estimate", C.c_double), ("pred_residual", C.c_double),
+                ("degree_scale", C.c_double), ("align_dot", C.c_double), ("signature", C.c_uint64),
+                ("nonfinite", C.c_int32), ("basis_used", C.c_int32)]
+
+
+class LsParams(C.Structure):
+    _fields_ = [("k", C.c_int32), ("first_slot", C.c_int32), ("max_iterations", C.c_int32),
+                ("subset_fraction", C.c_double),
+                ("final_sweep_fraction", C.c_double), ("final_sweep_iters", C.c_int32),
+                ("num_rounds", C.c_int32), ("seed", C.c_uint64)]
+
+
+class LsResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("final_passes", C.c_int32),
+                ("integer_gains", C.c_int32), ("total_flips", C.c_int64)]
+
+
+# name -> (restype, argtypes): every symbol include/specann_b200.h declares
+SIGNATURES = {
+    "sa_version": (C.c_char_p, []),
+    "sa_workspace_size": (C.c_int, [C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                    C.POINTER(C.c_size_t)]),
+    "sa_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
+                            C.c_int32, C.c_void_p, C.c_size_t, C.c_void_p]),
+    "sa_destroy": (C.c_int, [C.c_void_p]),
+    "sa_set_matrix": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
+                                C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
+    "sa_spmv_scaled": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
+    "sa_alpha_solve": (C.c_int, [C.c_void_p, C.POINTER(AlphaParams), C.POINTER(AlphaRecord)]),
+    "sa_result_vector": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "sa_commit_alpha": (C.c_int, [C.c_void_p]),
+    "sa_set_last_vector": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "sa_round_vector": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_int32, C.POINTER(C.c_uint64)]),
+    "sa_candidate_keep": (C.c_int, [C.c_void_p, C.c_int32]),
+    "sa_candidate_equal": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
+    "sa_candidate_set": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "sa_candidate_get": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
+    "sa_candidate_unpack": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
+    "sa_ls_workspace_size": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_size_t)]),
+    "sa_local_search": (C.c_int, [C.c_void_p, C.POINTER(LsParams), C.c_void_p, C.c_size_t,
+                                  C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(LsResult)]),
+    "sa_energies": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t, C.POINTER(C.c_double)]),
+}
+
+GRAPH_SIGNATURES = {
+    "sa_graph_ba_nnz": (C.c_int64, [C.c_int64, C.c_int64]),
+    "sa_graph_ba": (C.c_int, [C.c_int64, C.c_int64, C.c_uint64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sa_graph_er_nnz": (C.c_int64, [C.c_int64, C.c_double, C.c_uint64]),
+    "sa_graph_er": (C.c_int, [C.c_int64, C.c_double, C.c_uint64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+}
+
+_lib = None
+_glib = None
+
+
+class SpecAnnError(RuntimeError):
+    def __init__(self, fn, status):
+        super().__init__(f"{fn} failed with status {STATUS_NAMES.get(status, status)}")
+        self.status = status
+
+
+def load(path: Path = LIB_PATH):
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not Path(path).exists():
+            raise RuntimeError(f"{path} is missing: build it with `python -m specann_b200.build`")
+        lib = C.CDLL(str(path))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def load_graphs(path: Path = GRAPH_LIB_PATH):
+    global _glib
+    if _glib is None:
+        if not Path(path).exists():
+            raise RuntimeError(f"{path} is missing: build it with `python -m specann_b200.build`")
+        lib = C.CDLL(str(path))
+        for name, (res, args) in GRAPH_SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _glib = lib
+    return _glib
+
+
+def check(fn: str, status: int):
+    """Map a C-ABI status onto the exceptions of the reference (utils/failures.py, EigensolverBreakdown)."""
+    if status == SA_OK:
+        return
+    if status == SA_ERR_OOM:
+        raise SpecAnnOutOfMemory(f"{fn}: workspace too small (out of memory)")
+    if status in (SA_ERR_BREAKDOWN, SA_ERR_NONFINITE):
+        raise EigensolverBreakdown(f"{fn}: {STATUS_NAMES[status]}")
+    if status == SA_ERR_NOT_CONVERGED:
+        raise NumericalFailure(f"{fn}: not converged")
+    raise SpecAnnError(fn, status)

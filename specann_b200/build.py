@@ -1,0 +1,78 @@
+"""Build the native libraries in-tree (no GPU needed: nvcc cross-compiles for sm_100a).
+
+    python -m specann_b200.build            # both libraries
+    python -m specann_b200.build --verbose  # also print ptxas resource usage
+
+Outputs (next to this file):
+  libspecann_b200.so   CUDA kernels + the C-ABI of include/specann_b200.h (sm_100a only)
+  libspecann_graphs.so seeded synthetic graph generators (host C++, OpenMP)
+"""
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+CUDA_LIB = "libspecann_b200.so"
+GRAPH_LIB = "libspecann_graphs.so"
+CU_SOURCES = ["capi.cu", "alpha.cu", "ls.cu"]
+HEADERS = ["common.cuh", "handle.cuh", "spmv.cuh"]
+
+
+def nvcc_path() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(target: Path, sources) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(Path(s).stat().st_mtime > t for s in sources)
+
+
+def build_cuda(verbose: bool = False, force: bool = False) -> Path:
+    out = PKG / CUDA_LIB
+    srcs = [CSRC / s for s in CU_SOURCES]
+    deps = srcs + [CSRC / h for h in HEADERS] + [ROOT / "include" / "specann_b200.h"]
+    if not force and not _stale(out, deps):
+        return out
+    cmd = [nvcc_path(), "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+           "--extended-lambda", "-Xcompiler", "-fPIC", "-shared", "-o", str(out),
+           f"-I{ROOT / 'include'}"]
+    if verbose:
+        cmd += ["-Xptxas", "-v"]
+    cmd += [str(s) for s in srcs]
+    subprocess.run(cmd, check=True)
+    return out
+
+
+def build_graphs(force: bool = False) -> Path:
+    out = PKG / GRAPH_LIB
+    src = CSRC / "graphgen.cpp"
+    if not force and not _stale(out, [src]):
+        return out
+    cxx = shutil.which("g++") or "g++"
+    subprocess.run([cxx, "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", str(out), str(src)],
+                   check=True)
+    return out
+
+
+def build_all(verbose: bool = False, force: bool = False):
+    return build_graphs(force), build_cuda(verbose, force)
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    for p in build_all(a.verbose, a.force):
+        print(p)
+    sys.exit(0)

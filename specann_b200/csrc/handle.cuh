@@ -1,0 +1,123 @@
+// Host-side handle of the SpecAnn engine and the device control blocks of its kernels.
+#pragma once
+#include <cstdint>
+#include <cstddef>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace sa {
+
+// Control block of the alpha-solve kernel (device memory, part of the workspace).
+struct AlphaCtrl {
+  GridSync gs;
+  double a[kNcvMax];        // diagonal of the projected tridiagonal T
+  double b[kNcvMax];        // off-diagonal (b[i] couples basis vectors i and i + 1)
+  double h[kNcvMax];        // reorthogonalisation coefficients of the current step
+  double s[kNcvMax];        // Ritz coefficients (restart / final vector)
+  double theta;             // current smallest Ritz value
+  double inv_b;             // 1 / norm of the pending (unnormalised) vector w
+  double ww;                // ||w||^2 before the update of the current step
+  double scale;             // final normalisation and sign of y
+  double nrm_y;
+  double rr;                // squared true residual
+  int j;                    // index of the basis vector the next step creates
+  int action;               // next action of every CTA (see alpha kernel)
+  int iters;
+  int restarts;
+  int mode;                 // start mode in use
+  int test_pred;            // the next step is the predictor's residual test
+  int pass2;                // second reorthogonalisation pass in progress
+  int nonfinite;
+  int secant_sign;
+  int pad0;
+  double pred_residual;
+  int pred_accepted;
+  int status;
+  unsigned long long sig;   // order-independent hash of the packed spins
+  double degree_scale;
+  double align_dot;
+  double res_est;
+};
+
+// Control block of the local-search kernel.
+struct LsCtrl {
+  GridSync gs;
+  int phase;                // 0 main loop, 1 final sweep, 2 done
+  int it;                   // main-loop passes used
+  int round, sub;
+  int final_passes;
+  int pad;
+  long long stream;         // selection stream of the current pass
+  long long m;              // nodes selected in the current pass
+  long long wl_count;       // work-list entries of the current pass
+  long long total_flips;
+  unsigned int active[4];   // candidates that have not yet had a pass without a flip
+  long long counts[128];    // flips per candidate in the current pass
+};
+
+struct Layout {
+  size_t total = 0;
+  size_t off(size_t bytes) {
+    size_t o = total;
+    total += (bytes + 255) & ~size_t(255);
+    return o;
+  }
+};
+
+// Upper bounds of the SpMV work list for a matrix of n rows and nnz entries.
+constexpr int kSegRows = 96;     // rows per short segment at most
+constexpr int kSegElems = 512;   // entries per short segment (a segment is closed once it has more)
+
+inline long long max_items(long long n, long long nnz) {
+  return n / kSegRows + nnz / kSegElems + 2 * (nnz / (kShortMax + 1)) + nnz / kChunk + 8;
+}
+inline long long max_multichunk_rows(long long nnz) { return nnz / (kChunk + 1) + 1; }
+inline long long max_long_partials(long long nnz) { return nnz / kChunk + max_multichunk_rows(nnz) + 1; }
+
+}  // namespace sa
+
+struct sa_handle {
+  long long n = 0, nnz = 0;
+  int rp64 = 0, prec = 32, ncv_max = 33, max_cand = 128;
+  cudaStream_t stream = nullptr;
+  char* ws = nullptr;
+  size_t ws_bytes = 0;
+  // bound matrix (caller-owned device memory)
+  const void* rowptr = nullptr;
+  const int32_t* col = nullptr;
+  const void* val = nullptr;
+  bool bound = false;
+  double c = 0.0, dmin = 0.0, dmax = 0.0;
+  int integer_J = 0;
+  // workspace carve-out
+  long long ldv = 0;            // leading dimension of basis vectors (n rounded up to 64)
+  void* sigma = nullptr;        // D^{-1/2} / sqrt(c) for the current alpha (T)
+  float* ld = nullptr;          // log2 d (float)
+  double* deg = nullptr;        // absolute degrees (double)
+  void* V = nullptr;            // Lanczos basis, ncv_max x ldv (T)
+  void* w = nullptr;
+  void* u = nullptr;
+  void* yv[3] = {nullptr, nullptr, nullptr};
+  int iy_out = 0, iy_last = 1, iy_prev = 2;
+  bool has_last = false, has_prev = false;
+  sa::WorkItem* items = nullptr;
+  long long n_items = 0, cap_items = 0;
+  long long* mc_base = nullptr;
+  int* mc_count = nullptr;
+  long long n_mc = 0, cap_mc = 0;
+  void* long_part = nullptr;
+  long long cap_long_part = 0;
+  double* blk_part = nullptr;
+  int blk_part_width = 0;
+  sa::AlphaCtrl* actrl = nullptr;
+  double* red = nullptr;        // small reduction scratch (set-up kernels)
+  uint32_t* cand = nullptr;     // candidate store, max_cand x W
+  uint32_t* refined = nullptr;  // refined candidates, max_cand x W
+  uint32_t* scratch = nullptr;  // rounded spins of the last solve, W words
+  long long W = 0;              // words per packed candidate
+  int group = 8;                // lanes per short row in the SpMV
+  int sm_count = 0;
+  int max_blocks = 0;           // cooperative grid size cap for this device
+  int blocks = 0;               // grid size used by the persistent kernels
+};

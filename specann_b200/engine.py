@@ -1,0 +1,218 @@
+"""Device-side engine: one handle of libspecann_b200.so over torch-allocated device memory.
+
+torch provides device memory and the stream; all arithmetic runs in the library's kernels. The
+engine owns: the device CSR (row pointers int32 or int64, columns int32, couplings in the working
+precision), the handle workspace, and the local-search workspace.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import AlphaParams, AlphaRecord, LsParams, LsResult, check
+
+
+def _require_cuda():
+    if not torch.cuda.is_available():
+        raise RuntimeError("specann_b200 needs a CUDA device (there is no CPU fallback)")
+
+
+@dataclass
+class MatrixInfo:
+    c: float
+    d_min: float
+    d_max: float
+    integer: bool
+
+
+class Engine:
+    """A solver handle: workspace, bound matrix, candidate store."""
+
+    def __init__(self, n: int, nnz: int, precision: int = 32, ncv_max: int = 33, max_candidates: int = 128,
+                 device: Optional[torch.device] = None, stream: Optional[torch.cuda.Stream] = None):
+        _require_cuda()
+        self.lib = _lib.load()
+        self.n, self.nnz = int(n), int(nnz)
+        self.precision = int(precision)
+        self.rowptr64 = self.nnz > np.iinfo(np.int32).max
+        self.ncv_max = int(ncv_max)
+        self.max_candidates = int(max_candidates)
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.stream = stream if stream is not None else torch.cuda.current_stream(self.device)
+        self.vdtype = torch.float32 if self.precision == 32 else torch.float64
+        nbytes = C.c_size_t(0)
+        check("sa_workspace_size", self.lib.sa_workspace_size(self.n, self.nnz, int(self.rowptr64), self.precision,
+                                                              self.ncv_max, self.max_candidates, C.byref(nbytes)))
+        self.workspace = torch.empty(int(nbytes.value) + 256, dtype=torch.uint8, device=self.device)
+        base = self.workspace.data_ptr()
+        self._ws_ptr = (base + 255) & ~255
+        self._ws_bytes = int(nbytes.value)
+        h = C.c_void_p()
+        check("sa_create", self.lib.sa_create(C.byref(h), self.n, self.nnz, int(self.rowptr64), self.precision,
+                                              self.ncv_max, self.max_candidates, C.c_void_p(self._ws_ptr),
+                                              self._ws_bytes, C.c_void_p(self.stream.cuda_stream)))
+        self.h = h
+        self.ls_workspace = None
+        self.info: Optional[MatrixInfo] = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sa_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- matrix -----------------------------------------------------------------------------
+    def upload_csr(self, indptr: np.ndarray, indices: np.ndarray, data: np.ndarray) -> MatrixInfo:
+        """H2D copy of a host CSR and the prelude (degrees, c, d, work list)."""
+        rp_dtype = np.int64 if self.rowptr64 else np.int32
+        val_dtype = np.float32 if self.precision == 32 else np.float64
+        self.d_rowptr = torch.from_numpy(np.ascontiguousarray(indptr, dtype=rp_dtype)).to(self.device, non_blocking=False)
+        self.d_col = torch.from_numpy(np.ascontiguousarray(indices, dtype=np.int32)).to(self.device)
+        self.d_val = torch.from_numpy(np.ascontiguousarray(data, dtype=val_dtype)).to(self.device)
+        return self.bind(self.d_rowptr, self.d_col, self.d_val)
+
+    def bind(self, rowptr: torch.Tensor, col: torch.Tensor, val: torch.Tensor) -> MatrixInfo:
+        """Bind device CSR tensors (kept alive by the engine) and run the prelude."""
+        self.d_rowptr, self.d_col, self.d_val = rowptr, col, val
+        c = C.c_double()
+        dmin = C.c_double()
+        dmax = C.c_double()
+        integer = C.c_int32()
+        check("sa_set_matrix", self.lib.sa_set_matrix(self.h, C.c_void_p(rowptr.data_ptr()), C.c_void_p(col.data_ptr()),
+                                                      C.c_void_p(val.data_ptr()), C.byref(c), C.byref(dmin),
+                                                      C.byref(dmax), C.byref(integer)))
+        self.info = MatrixInfo(c=c.value, d_min=dmin.value, d_max=dmax.value, integer=bool(integer.value))
+        return self.info
+
+    # ---- operator ---------------------------------------------------------------------------
+    def spmv(self, alpha: float, rho: float, x: torch.Tensor, y: Optional[torch.Tensor] = None) -> torch.Tensor:
+        if y is None:
+            y = torch.empty_like(x)
+        check("sa_spmv_scaled", self.lib.sa_spmv_scaled(self.h, float(alpha), float(rho), C.c_void_p(x.data_ptr()),
+                                                        C.c_void_p(y.data_ptr())))
+        return y
+
+    # ---- one alpha --------------------------------------------------------------------------
+    def alpha_solve(self, *, alpha, alpha_prev, rho, gershgorin, tol, pred_tol, maxiter, ncv, start_mode,
+                    seed, stream_id, align=True, v0: Optional[torch.Tensor] = None, secant_gamma=1.0,
+                    round_spins=True, residual_check=True) -> AlphaRecord:
+        p = AlphaParams(alpha=float(alpha), alpha_prev=float(alpha_prev), rho=float(rho),
+                        gershgorin=float(gershgorin), tol=float(tol), pred_tol=float(pred_tol),
+                        secant_gamma=float(secant_gamma), maxiter=int(maxiter), ncv=int(ncv),
+                        start_mode=int(start_mode), align=int(bool(align)), seed=int(seed) & (2 ** 64 - 1),
+                        stream_id=int(stream_id), v0=C.c_void_p(v0.data_ptr()) if v0 is not None else None,
+                        round=int(bool(round_spins)), residual_check=int(bool(residual_check)))
+        rec = AlphaRecord()
+        check("sa_alpha_solve", self.lib.sa_alpha_solve(self.h, C.byref(p), C.byref(rec)))
+        return rec
+
+    def result_vector(self) -> torch.Tensor:
+        """A copy of the last solve's eigenvector y (device)."""
+        ptr = C.c_void_p()
+        check("sa_result_vector", self.lib.sa_result_vector(self.h, C.byref(ptr)))
+        return device_view(ptr.value, self.n, self.vdtype, self.device).clone()
+
+    def commit(self):
+        check("sa_commit_alpha", self.lib.sa_commit_alpha(self.h))
+
+    def set_last_vector(self, y: torch.Tensor):
+        check("sa_set_last_vector", self.lib.sa_set_last_vector(self.h, C.c_void_p(y.data_ptr())))
+
+    def round_vector(self, alpha: float, y: torch.Tensor, align: bool = True) -> int:
+        sig = C.c_uint64()
+        check("sa_round_vector", self.lib.sa_round_vector(self.h, float(alpha), C.c_void_p(y.data_ptr()),
+                                                          int(bool(align)), C.byref(sig)))
+        return int(sig.value)
+
+    # ---- candidates -------------------------------------------------------------------------
+    def keep_candidate(self, slot: int):
+        check("sa_candidate_keep", self.lib.sa_candidate_keep(self.h, int(slot)))
+
+    def candidate_equal(self, slot: int) -> bool:
+        eq = C.c_int32()
+        check("sa_candidate_equal", self.lib.sa_candidate_equal(self.h, int(slot), C.byref(eq)))
+        return bool(eq.value)
+
+    def set_candidate(self, slot: int, spins: np.ndarray):
+        words = torch.from_numpy(pack_words(spins).view(np.int32)).to(self.device)
+        check("sa_candidate_set", self.lib.sa_candidate_set(self.h, int(slot), C.c_void_p(words.data_ptr())))
+        self.stream.synchronize()
+
+    def candidate_words(self, slot: int, refined: bool = False) -> np.ndarray:
+        W = (self.n + 31) // 32
+        out = torch.empty(W, dtype=torch.int32, device=self.device)
+        check("sa_candidate_get", self.lib.sa_candidate_get(self.h, int(slot), int(refined), C.c_void_p(out.data_ptr())))
+        return out.cpu().numpy().view(np.uint32)
+
+    def candidate_spins(self, slot: int, refined: bool = False) -> torch.Tensor:
+        out = torch.empty(self.n, dtype=torch.int8, device=self.device)
+        check("sa_candidate_unpack", self.lib.sa_candidate_unpack(self.h, int(slot), int(refined),
+                                                                  C.c_void_p(out.data_ptr())))
+        return out
+
+    # ---- local search and energies -----------------------------------------------------------
+    def _ls_ws(self, k: int):
+        nbytes = C.c_size_t(0)
+        check("sa_ls_workspace_size", self.lib.sa_ls_workspace_size(self.h, int(k), C.byref(nbytes)))
+        need = int(nbytes.value) + 256
+        if self.ls_workspace is None or self.ls_workspace.numel() < need:
+            self.ls_workspace = torch.empty(need, dtype=torch.uint8, device=self.device)
+        base = self.ls_workspace.data_ptr()
+        return (base + 255) & ~255, int(nbytes.value)
+
+    def local_search(self, k: int, *, first_slot=0, max_iterations=1000, subset_fraction=0.9,
+                     final_sweep_fraction=1.0, final_sweep_iters=25, num_rounds=25, seed=0):
+        ptr, nbytes = self._ls_ws(k)
+        p = LsParams(k=int(k), first_slot=int(first_slot), max_iterations=int(max_iterations),
+                     subset_fraction=float(subset_fraction),
+                     final_sweep_fraction=float(final_sweep_fraction), final_sweep_iters=int(final_sweep_iters),
+                     num_rounds=int(num_rounds), seed=int(seed) & (2 ** 64 - 1))
+        eb = (C.c_double * k)()
+        ea = (C.c_double * k)()
+        res = LsResult()
+        check("sa_local_search", self.lib.sa_local_search(self.h, C.byref(p), C.c_void_p(ptr), nbytes, eb, ea,
+                                                          C.byref(res)))
+        return np.array(eb[:]), np.array(ea[:]), res
+
+    def energies(self, k: int) -> np.ndarray:
+        ptr, nbytes = self._ls_ws(k)
+        e = (C.c_double * k)()
+        check("sa_energies", self.lib.sa_energies(self.h, int(k), C.c_void_p(ptr), nbytes, e))
+        return np.array(e[:])
+
+
+class _CudaArray:
+    """Minimal __cuda_array_interface__ holder for a raw device pointer."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+_TYPESTR = {torch.float32: "<f4", torch.float64: "<f8", torch.int8: "|i1", torch.int32: "<i4",
+            torch.uint8: "|u1", torch.int64: "<i8"}
+
+
+def device_view(ptr: int, n: int, dtype: torch.dtype, device) -> torch.Tensor:
+    """Zero-copy torch view of n elements at a device pointer owned by the engine's workspace."""
+    return torch.as_tensor(_CudaArray(ptr, n, _TYPESTR[dtype]), device=device)
+
+
+def pack_words(spins: np.ndarray) -> np.ndarray:
+    """Device layout of a rounded candidate: bit (j % 32) of uint32 word j // 32 is 1 iff s_j > 0."""
+    s = np.asarray(spins)
+    n = s.size
+    nw = (n + 31) // 32
+    bits = np.zeros(nw * 32, dtype=np.uint64)
+    bits[:n] = s > 0
+    return (bits.reshape(nw, 32) << np.arange(32, dtype=np.uint64)).sum(axis=1).astype(np.uint32)

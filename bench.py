@@ -1,0 +1,321 @@
+"""Benchmark: seconds per 128-alpha SpecAnn solve on a Barabasi-Albert graph (default n = 2^20, m = 20,
+J = -A, fp32 couplings, int32 columns), the paper's SpecAnn run (sqrt schedule, diagonal predictor,
+eigsh tolerance 1e-6, batched local search), plus the fused SpMV's HBM bandwidth.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--log2n 20] [--m 20]
+
+A step is one full solve (prelude, 128 eigensolves, rounding, deduplication, batched local search,
+best candidate). `value` is timed with the CSR already in HBM (SpectralAnnealing.solve_device);
+`e2e` is the same metric through SpectralAnnealing.solve(J) with a host SciPy CSR, so every step
+includes the host-to-device copy of the matrix and the device-to-host copy of the best spins.
+Under torchrun each rank solves its own seed of the same graph (independent replicas, no collective
+on the data path); `value` is the max-over-ranks step time divided by the number of solves.
+
+--impl reference times the CPU reference pipeline (the oracle port: SciPy ARPACK eigsh + NumPy local
+search) on a bounded sample of the same workload and extrapolates to a full 128-alpha solve.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "s per 128-alpha SpecAnn solve (BA m=20, sqrt schedule, FP32 + FP64 Ritz); SpMV HBM GB/s"
+UNIT = "s/solve"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--log2n", type=int, default=20)
+    ap.add_argument("--m", type=int, default=20)
+    ap.add_argument("--num-alphas", type=int, default=128)
+    ap.add_argument("--precision", type=int, default=32)
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-alphas", type=int, default=2)
+    ap.add_argument("--spmv-reps", type=int, default=20)
+    return ap.parse_args()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"specann_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        try:
+            self.path.unlink()
+        except Exception:
+            pass
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_graph(args, seed=42):
+    from specann_b200 import graphs
+    n = 1 << args.log2n
+    rowptr, col, val = graphs.barabasi_albert_arrays(n, args.m, seed=seed, couplings="unit")
+    return n, rowptr, col, val
+
+
+def spmv_bytes(n, nnz, rp_bytes, t):
+    """Algorithmic bytes of one fused SpMV: nnz (col + value) + (n+1) row pointers + x, s, y."""
+    return nnz * (4 + t) + (n + 1) * rp_bytes + 3 * n * t
+
+
+def run_reference(args, rank, world):
+    """CPU reference pipeline (oracle port) on a bounded sample, extrapolated to one full solve."""
+    if rank != 0:
+        return
+    import scipy.sparse as sp
+    from oracle import specann_oracle as O
+    n, rowptr, col, val = make_graph(args)
+    J = sp.csr_matrix((val.astype(np.float64), col, rowptr.astype(np.int32 if rowptr[-1] < 2**31 else np.int64)),
+                      shape=(n, n))
+    k = args.cpu_sample_alphas
+    scale = args.num_alphas / k
+    sample = f"{k} consecutive warm-started alphas of {args.num_alphas} + local search of their candidates, x{scale:g}"
+    times = []
+    for step in range(args.warmup + args.steps):
+        start_idx = (step * k) % args.num_alphas
+        t0 = time.perf_counter()
+        O.solve(J, precision=args.precision, num_alphas=args.num_alphas, seed=42 + step,
+                alpha_subset=list(range(start_idx, start_idx + k)))
+        dt = (time.perf_counter() - t0) * scale
+        if step >= args.warmup:
+            times.append(dt)
+    value = float(np.mean(times))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": value * 1000.0, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == 32 else "f64",
+            "data": "synthetic (seeded BA generator)", "impl": "reference",
+            "config": {"workload": f"BA(n=2^{args.log2n}, m={args.m}) J=-A, {args.num_alphas} alphas sqrt schedule",
+                       "n": n, "nnz": int(rowptr[-1])},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def cpu_baseline_sample(args, n, rowptr, col, val):
+    import scipy.sparse as sp
+    from oracle import specann_oracle as O
+    J = sp.csr_matrix((val.astype(np.float64), col, rowptr.astype(np.int32 if rowptr[-1] < 2**31 else np.int64)),
+                      shape=(n, n))
+    k = args.cpu_sample_alphas
+    t0 = time.perf_counter()
+    O.solve(J, precision=args.precision, num_alphas=args.num_alphas, seed=42, alpha_subset=list(range(k)))
+    dt = time.perf_counter() - t0
+    scale = args.num_alphas / k
+    return {"value": dt * scale, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{k} warm-started alphas of {args.num_alphas} + local search of their candidates "
+                      f"({dt:.1f} s measured), x{scale:g}; SciPy ARPACK eigsh and NumPy, single-threaded"}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+    from specann_b200 import _lib
+    from specann_b200.spectral_annealing import SpectralAnnealing
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    lib = _lib.load()
+    n, rowptr, col, val = make_graph(args)
+    nnz = int(rowptr[-1])
+    rp_np = rowptr.astype(np.int32) if nnz < 2**31 else rowptr
+    import scipy.sparse as sp
+    J_host = sp.csr_matrix((val.astype(np.float64) if args.precision == 64 else val, col, rp_np), shape=(n, n))
+    d_rowptr = torch.from_numpy(rp_np).to(dev)
+    d_col = torch.from_numpy(col).to(dev)
+    d_val = torch.from_numpy(val if args.precision == 32 else val.astype(np.float64)).to(dev)
+    t = 4 if args.precision == 32 else 8
+    seed = 42 + rank
+
+    def solver(profile=False):
+        return SpectralAnnealing("bench.txt", "bench", random_seed=seed, num_alphas=args.num_alphas,
+                                 precision=args.precision, write_results=False, profile=profile)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up (untimed), then K timed steps with the CSR resident in HBM
+    for _ in range(args.warmup):
+        solver().solve_device(d_rowptr, d_col, d_val)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    stream = torch.cuda.current_stream()
+    launches0 = lib.sa_kernel_launches()
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    energies = []
+    for _ in range(args.steps):
+        e, _, _ = solver().solve_device(d_rowptr, d_col, d_val)
+        energies.append(e)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = lib.sa_kernel_launches() - launches0
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = ms / 1000.0 / world
+
+    # one profiled solve: per-kernel event times and algorithmic bytes of the alpha kernels
+    s = solver(profile=True)
+    s.solve_device(d_rowptr, d_col, d_val)
+    st = s.engine.stats
+    iters = np.array([r["eigsh_iterations"] for r in s.alpha_results], dtype=np.float64)
+    if os.environ.get("SPECANN_BENCH_DUMP"):
+        with open(os.environ["SPECANN_BENCH_DUMP"], "w") as f:
+            for r in s.alpha_results:
+                f.write(json.dumps({k: r[k] for k in ("alpha", "eigsh_iterations", "eigsh_restarts", "eigsh_residual",
+                                                      "lambda1", "pred_accepted", "pred_residual", "candidate")}) + "\n")
+    lanczos = {"mean": float(iters.mean()), "median": float(np.median(iters)), "max": float(iters.max()),
+               "alpha0": float(iters[0]), "restarts": int(sum(r["eigsh_restarts"] for r in s.alpha_results)),
+               "pred_accepted": int(sum(1 for r in s.alpha_results if r["pred_accepted"])),
+               "max_residual": float(np.nanmax([r["eigsh_residual"] for r in s.alpha_results])),
+               "candidates": int(s._num_candidates or 0)}
+    hbm, peak_kind = peaks()
+    alpha_gbs = st["alpha_bytes"] / (st["alpha_ms"] / 1000.0) / 1e9 if st["alpha_ms"] > 0 else None
+
+    # standalone fused SpMV (the north-star SpMV bandwidth figure): K launches on resident data
+    from specann_b200.engine import Engine
+    eng = Engine(n, nnz, precision=args.precision, ncv_max=33, max_candidates=1)
+    eng.bind(d_rowptr, d_col, d_val)
+    x = torch.randn(n, device=dev, dtype=torch.float32 if args.precision == 32 else torch.float64)
+    y = torch.empty_like(x)
+    for _ in range(3):
+        eng.spmv(0.5, 1.001, x, y)
+    torch.cuda.synchronize()
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(args.spmv_reps):
+        eng.spmv(0.5, 1.001, x, y)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    spmv_ms = s0.elapsed_time(s1) / args.spmv_reps   # includes the O(n) scale kernel of each call
+    sb = spmv_bytes(n, nnz, rp_np.itemsize, t)
+    spmv_gbs = sb / (spmv_ms / 1000.0) / 1e9
+
+    # e2e: the public API with a host SciPy CSR (H2D of the matrix and D2H of the spins inside)
+    e2e_steps = args.e2e_steps or max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        solver().solve(J_host)
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if world > 1:
+        tt = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    h2d = int(rp_np.nbytes + col.nbytes + nnz * (4 if args.precision == 32 else 8))
+    d2h = int(n * t)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if args.precision == 32 else "f64",
+        "data": "synthetic (seeded BA generator, J = -A)",
+        "config": {"workload": f"BA(n=2^{args.log2n}, m={args.m}) J=-A, {args.num_alphas} alphas sqrt schedule, "
+                               f"diagonal predictor, eigsh_tol 1e-6, batched local search",
+                   "n": n, "nnz": nnz, "precision": args.precision, "replicas": world,
+                   "l2": "inputs larger than L2 (CSR %.0f MB > 126 MB)" % ((rp_np.nbytes + col.nbytes + nnz * t) / 1e6),
+                   "best_energy": float(energies[-1]) if energies else None},
+        "e2e": {"value": e2e_s / world, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "achieved": alpha_gbs, "peak": hbm, "unit": "GB/s",
+                     "frac": (alpha_gbs / hbm) if alpha_gbs else None, "traffic": None,
+                     "kernel": "alpha_kernel (persistent: fused SpMV + Lanczos + rounding)",
+                     "peak_source": peak_kind,
+                     "alpha_kernel_ms_per_solve": st["alpha_ms"], "alpha_launches_per_solve": st["alpha_launches"],
+                     "spmvs_per_solve": st["spmvs"], "ls_kernel_ms_per_solve": st["ls_ms"],
+                     "lanczos_iterations": lanczos},
+        "spmv": {"achieved": spmv_gbs, "peak": hbm, "unit": "GB/s", "frac": spmv_gbs / hbm,
+                 "ms": spmv_ms, "bytes": sb},
+        "clocks": clk,
+        "gpu_launches": int(launches),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(args, n, rowptr, col, val)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

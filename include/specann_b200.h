@@ -76,6 +76,9 @@ typedef struct {
   uint64_t signature;    /* 64-bit hash of the packed rounded spins */
   int32_t nonfinite;     /* 1 if the eigenvector had a non-finite entry */
   int32_t basis_used;    /* basis vectors in use at the end */
+  int32_t spmv_count;    /* fused SpMVs the launch ran (Lanczos steps, predictor test, residual) */
+  int32_t reserved;
+  double alg_bytes;      /* algorithmic DRAM bytes of the launch: SpMVs + basis/vector passes */
 } sa_alpha_record;
 
 typedef struct {
@@ -87,6 +90,8 @@ typedef struct {
   int32_t final_sweep_iters;    /* 25 */
   int32_t num_rounds;           /* 25 */
   uint64_t seed;                /* node-selection stream seed */
+  int32_t semantics;            /* 0: priority passes (default), 1: snapshot (Jacobi) passes */
+  int32_t reserved;
 } sa_ls_params;
 
 typedef struct {
@@ -172,6 +177,10 @@ int sa_energies(sa_handle* h, int32_t k, void* ls_workspace, size_t ls_bytes, do
 
 /* Version string of the library. */
 const char* sa_version(void);
+
+/* Kernel launches this library has issued since it was loaded (diagnostics; no reference
+ * counterpart). */
+uint64_t sa_kernel_launches(void);
 
 #ifdef __cplusplus
 }

@@ -12,12 +12,18 @@ iteration trajectory.
 
 Local search: the reference kernel updates spins in place from concurrent warps
 (models/spectral_annealing.py:821-869), so its result depends on thread timing. This project
-defines the local search as snapshot (Jacobi) passes: within a pass every selected node decides from
-the spins at the start of the pass, and all decided flips are applied together. Node selection uses
-the counter-based stream of ``oracle.selection``. ``local_search`` is that definition; the CUDA
-kernel must match it bit for bit for integer couplings. ``reference_kernel_pass`` restates the
-reference kernel's own arithmetic (fp32 lane-strided partial sums and shuffle tree, in-place
-updates in warp order) so that differences can be counted.
+defines two deterministic pass semantics over the same node-selection stream (``oracle.selection``),
+both decided from the spins at the start of the pass:
+  * "priority" (default): a selected node that wants to flip (2 s_i (J s)_i < 0) flips unless a
+    neighbour that also wants to flip comes earlier in the pass's permutation. The flips of a pass
+    form an independent set, so each one lowers the energy by exactly its gain: the pass equals a
+    sequential sweep of single flips (the in-order schedule of the reference kernel, with the blocked
+    nodes deferred to the next pass). Energy decreases monotonically.
+  * "snapshot": every wanting node flips (Jacobi). Adjacent nodes can flip together and undo each
+    other, so on dense or large graphs it can oscillate and raise the energy.
+``local_search`` implements both; the CUDA kernel matches it bit for bit for integer couplings.
+``reference_kernel_pass`` restates the reference kernel's own arithmetic (fp32 lane-strided partial
+sums and shuffle tree, in-place updates in warp order) so that differences can be counted.
 """
 from __future__ import annotations
 
@@ -326,16 +332,21 @@ def is_integer_matrix(J) -> bool:
 
 def local_search(J, spins_kn, seed: int, max_iterations: int = 1000, subset_fraction: float = 0.9,
                  final_sweep_fraction: float = 1.0, final_sweep_iters: int = 25,
-                 num_rounds: int = 25) -> LSResult:
-    """Snapshot-pass batched local search with the control flow of flip_refinement and
-    gpu_final_sweep (models/spectral_annealing.py:1039-1112, :983-1036).
+                 num_rounds: int = 25, semantics: str = "priority") -> LSResult:
+    """Batched local search with the control flow of flip_refinement and gpu_final_sweep
+    (models/spectral_annealing.py:1039-1112, :983-1036).
 
-    A pass over the selected nodes flips every (node, candidate) whose energy change
-    2 s_i (J s)_i is negative, all decided from the spins at the start of the pass. The main loop
-    stops when every candidate has had a pass without a flip (sticky mask, :1096-1100) or after
-    max_iterations passes; then num_rounds rounds of up to final_sweep_iters passes, each round
-    ending at the first pass in which no candidate flips (:1023-1034).
+    A pass over the selected nodes decides, from the spins at the start of the pass, which
+    (node, candidate) pairs want to flip (energy change 2 s_i (J s)_i < 0); with "priority" a wanting
+    node is held back when a wanting neighbour has a lower rank in the pass's permutation, with
+    "snapshot" every wanting node flips. A candidate has a flip in a pass iff it has a wanting node
+    (the lowest-ranked wanting node is never held back), so the stopping rules are those of the
+    reference: the main loop stops when every candidate has had a pass without a flip (sticky mask,
+    :1096-1100) or after max_iterations passes; then num_rounds rounds of up to final_sweep_iters
+    passes, each round ending at the first pass in which no candidate flips (:1023-1034).
     """
+    if semantics not in ("priority", "snapshot"):
+        raise ValueError(semantics)
     S = np.asarray(spins_kn, dtype=np.int64).T.copy()      # n x k
     n, k = S.shape
     integer = is_integer_matrix(J)
@@ -348,10 +359,16 @@ def local_search(J, spins_kn, seed: int, max_iterations: int = 1000, subset_frac
     e_before = -(S * H).sum(axis=0)
     e_before = e_before // 2 if integer else 0.5 * e_before
     total = [0]
+    coo = sp.csr_matrix(J).tocoo()
 
-    def one_pass(sel):
+    def one_pass(sel, rank):
         nonlocal S, H
         dec = ((S * H) < 0) & sel[:, None]
+        if semantics == "priority" and dec.any():
+            earlier = rank[coo.col] < rank[coo.row]
+            P = sp.csr_matrix((np.ones(int(earlier.sum())), (coo.row[earlier], coo.col[earlier])), shape=J.shape)
+            blocked = (P @ dec.astype(np.float64)) > 0
+            dec = dec & ~blocked
         counts = dec.sum(axis=0)
         if dec.any():
             dS = np.where(dec, -2 * S, 0)
@@ -365,15 +382,17 @@ def local_search(J, spins_kn, seed: int, max_iterations: int = 1000, subset_frac
     m_main = selection.num_selected(n, subset_fraction)
     for it in range(int(max_iterations)):
         used += 1
-        counts = one_pass(selection.selected_mask(n, seed, it, m_main))
+        rank = selection.ranks(n, seed, it)
+        counts = one_pass(rank < m_main, rank)
         active &= counts > 0
         if not active.any():
             break
     m_final = selection.num_selected(n, final_sweep_fraction)
     for r in range(int(num_rounds)):
-        sel = selection.selected_mask(n, seed, selection.FINAL_STREAM_BASE + r, m_final)
+        rank = selection.ranks(n, seed, selection.FINAL_STREAM_BASE + r)
+        sel = rank < m_final
         for _ in range(int(final_sweep_iters)):
-            counts = one_pass(sel)
+            counts = one_pass(sel, rank)
             if not (counts > 0).any():
                 break
     e_after = -(S * H).sum(axis=0)
@@ -433,7 +452,7 @@ class SolveResult:
 def solve(J, *, precision=32, schedule="sqrt", num_alphas=128, schedule_interval=(0.0, 1.0),
           pred_mode="diagonal", pred_tol=1e-3, shift_eps=1e-3, eigsh_tol=1e-6, eigsh_maxiter=1000,
           eigsh_ncv=None, disable_warm_start=False, use_local_search=True, max_local_iterations=1000,
-          seed=42, alpha_subset=None) -> SolveResult:
+          seed=42, alpha_subset=None, ls_semantics="priority", energy_mode="exact") -> SolveResult:
     """models/spectral_annealing.py:262-525 with SciPy eigsh and the snapshot local search.
 
     ``alpha_subset`` (indices into the schedule) runs only those alphas, in order, as a bounded
@@ -464,8 +483,12 @@ def solve(J, *, precision=32, schedule="sqrt", num_alphas=128, schedule_interval
         if key not in uniq:
             uniq[key] = len(cand_list)
             cand_list.append(spins)
-        raw = float(fp32_energies(pre.Js, spins[None, :], pre.c)[0]) if precision == 32 else \
-            float(-0.5 * pre.c * spins.astype(np.float64) @ (pre.Js @ spins.astype(np.float64)))
+        if energy_mode == "exact":
+            raw = exact_energy(J, spins)
+        elif precision == 32:
+            raw = float(fp32_energies(pre.Js, spins[None, :], pre.c)[0])
+        else:
+            raw = float(-0.5 * pre.c * spins.astype(np.float64) @ (pre.Js @ spins.astype(np.float64)))
         records.append(dict(alpha=alpha, lambda1=res.lambda1, rho=res.rho, candidate=uniq[key],
                             raw_energy=raw, energy=raw, pred_residual=res.pred_residual,
                             pred_accepted=res.pred_accepted, retry=res.retry, residual=res.residual))
@@ -473,7 +496,8 @@ def solve(J, *, precision=32, schedule="sqrt", num_alphas=128, schedule_interval
             best_e, best_s, best_a = raw, spins.copy(), alpha
     ls = None
     if use_local_search and cand_list:
-        ls = local_search(J, np.stack(cand_list), seed=seed, max_iterations=max_local_iterations)
+        ls = local_search(J, np.stack(cand_list), seed=seed, max_iterations=max_local_iterations,
+                          semantics=ls_semantics)
         for rec in records:
             c = rec["candidate"]
             orig = rec["raw_energy"]

@@ -43,14 +43,16 @@ class AlphaRecord(C.Structure):
                 ("pred_accepted", C.c_int32), ("mu", C.c_double), ("lambda1", C.c_double),
                 ("residual", C.c_double), ("res_estimate", C.c_double), ("pred_residual", C.c_double),
                 ("degree_scale", C.c_double), ("align_dot", C.c_double), ("signature", C.c_uint64),
-                ("nonfinite", C.c_int32), ("basis_used", C.c_int32)]
+                ("nonfinite", C.c_int32), ("basis_used", C.c_int32), ("spmv_count", C.c_int32),
+                ("reserved", C.c_int32), ("alg_bytes", C.c_double)]
 
 
 class LsParams(C.Structure):
     _fields_ = [("k", C.c_int32), ("first_slot", C.c_int32), ("max_iterations", C.c_int32),
                 ("subset_fraction", C.c_double),
                 ("final_sweep_fraction", C.c_double), ("final_sweep_iters", C.c_int32),
-                ("num_rounds", C.c_int32), ("seed", C.c_uint64)]
+                ("num_rounds", C.c_int32), ("seed", C.c_uint64), ("semantics", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class LsResult(C.Structure):
@@ -61,6 +63,7 @@ class LsResult(C.Structure):
 # name -> (restype, argtypes): every symbol include/specann_b200.h declares
 SIGNATURES = {
     "sa_version": (C.c_char_p, []),
+    "sa_kernel_launches": (C.c_uint64, []),
     "sa_workspace_size": (C.c_int, [C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                     C.POINTER(C.c_size_t)]),
     "sa_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int32,

@@ -3,6 +3,9 @@
 // FP64 inner products and an FP64 tridiagonal Ritz solve, the Ritz-matrix guard, sign alignment,
 // the true residual, and rounding to packed spins with an order-independent signature.
 //
+// CTAs rewrite V, w, u and y between phases and the per-SM L1 is not coherent with writes from
+// other SMs, so every read of those arrays inside this kernel uses ld.global.cg (L2).
+//
 // Vectors (basis V, w, u, y) are in T (float or double); every inner product and norm is
 // accumulated in double; the projected tridiagonal T_j lives in double in the control block.
 // Between phases the CTAs meet at grid_barrier, whose epilogue (run by the last CTA to arrive)
@@ -17,6 +20,8 @@
 
 namespace sa {
 
+void count_launches(int k);
+
 enum Action : int { ACT_NEXT = 0, ACT_REPASS = 1, ACT_RESTART = 2, ACT_REJECT = 3, ACT_DONE = 4, ACT_ERROR = 5,
                     ACT_P0_AGAIN = 6 };
 
@@ -28,7 +33,7 @@ struct AlphaArgs {
   SpmvArgs<T, RP> S;
   long long n, ldv;
   T* sigma;
-  const float* ld;
+  const double* ld;
   T* V;
   T* w;
   T* u;
@@ -46,6 +51,8 @@ struct AlphaArgs {
   double half_log2_c;
   double sqrt_c;
   int group;
+  double spmv_bytes;     // algorithmic bytes of one fused SpMV
+  double* dense;         // implicit-restart scratch (dense T, then dense Q)
 };
 
 // ---- small dense helpers for the projected tridiagonal (double, one CTA) --------------------
@@ -190,6 +197,86 @@ __device__ void tridiag_eigvec(const double* a, const double* b, int m, double t
   }
 }
 
+// The (q+1)-th smallest eigenvalue of the tridiagonal by bisection on the Sturm count.
+__device__ double kth_eig(const double* a, const double* b, int m, int q) {
+  double lo = 1e300, hi = -1e300;
+  for (int i = 0; i < m; ++i) {
+    const double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i + 1 < m ? fabs(b[i]) : 0.0);
+    lo = fmin(lo, a[i] - r);
+    hi = fmax(hi, a[i] + r);
+  }
+  lo -= 1e-12 * fmax(1.0, fabs(lo));
+  hi += 1e-12 * fmax(1.0, fabs(hi));
+  for (int it = 0; it < 80 && hi - lo > 1e-15 * fmax(1.0, fabs(hi)); ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (sturm_count(a, b, m, mid) >= q + 1) hi = mid;
+    else lo = mid;
+  }
+  return 0.5 * (lo + hi);
+}
+
+// Implicit restart with exact shifts (the CTA): the m - kk largest Ritz values of the tridiagonal
+// (a, b; size m) are the shifts of implicit QR steps, done as Givens bulge chasing on a dense copy
+// Td with the rotations accumulated in Qd (both m x m, row-major). Afterwards Qd^T T Qd has a
+// leading kk x kk tridiagonal, written back to a and b, and the residual of the kept basis is
+// V Q[:, kk] T+[kk][kk-1] + w Q[m-1][kk-1] (w: the pending unnormalised Lanczos vector).
+__device__ void implicit_restart(AlphaCtrl* C, double* Td, double* Qd, int m, int kk) {
+  __shared__ double s_ritz[kNcvMax];
+  __shared__ double s_c, s_s;
+  const int t = threadIdx.x;
+  if (t < m) s_ritz[t] = kth_eig(C->a, C->b, m, t);
+  for (int idx = t; idx < m * m; idx += blockDim.x) {
+    const int r = idx / m, c = idx % m;
+    double v = 0.0;
+    if (r == c) v = C->a[r];
+    else if (r == c + 1) v = C->b[c];
+    else if (c == r + 1) v = C->b[r];
+    Td[idx] = v;
+    Qd[idx] = (r == c) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  for (int sft = m - 1; sft >= kk; --sft) {
+    const double mu = s_ritz[sft];
+    for (int r = 0; r < m - 1; ++r) {
+      if (t == 0) {
+        const double x = (r == 0) ? Td[0] - mu : Td[r * m + (r - 1)];
+        const double z = (r == 0) ? Td[m] : Td[(r + 1) * m + (r - 1)];
+        const double rr = hypot(x, z);
+        s_c = (rr == 0.0) ? 1.0 : x / rr;
+        s_s = (rr == 0.0) ? 0.0 : z / rr;
+      }
+      __syncthreads();
+      const double c = s_c, s = s_s;
+      if (t < m) {
+        const double p = Td[r * m + t], q = Td[(r + 1) * m + t];
+        Td[r * m + t] = c * p + s * q;
+        Td[(r + 1) * m + t] = -s * p + c * q;
+      }
+      __syncthreads();
+      if (t < m) {
+        double p = Td[t * m + r], q = Td[t * m + r + 1];
+        Td[t * m + r] = c * p + s * q;
+        Td[t * m + r + 1] = -s * p + c * q;
+        p = Qd[t * m + r];
+        q = Qd[t * m + r + 1];
+        Qd[t * m + r] = c * p + s * q;
+        Qd[t * m + r + 1] = -s * p + c * q;
+      }
+      __syncthreads();
+    }
+  }
+  if (t < kk) {
+    C->a[t] = Td[t * m + t];
+    if (t + 1 < kk) C->b[t] = Td[(t + 1) * m + t];
+  }
+  if (t == 0) {
+    C->irl_beta = Td[kk * m + (kk - 1)];
+    C->irl_sigma = Qd[(m - 1) * m + (kk - 1)];
+    C->irl_k = kk;
+  }
+  __syncthreads();
+}
+
 // ---- reductions of per-CTA partials --------------------------------------------------------
 
 // Sum part[blk * pw + col] over blocks for cols [0, ncols) into out[col] (fixed order).
@@ -235,10 +322,12 @@ __device__ __forceinline__ unsigned long long word_mix(long long widx, unsigned 
 // ---- the alpha-solve kernel ----------------------------------------------------------------
 
 template <typename T, typename RP>
-__global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
+__global__ void __launch_bounds__(kThreads, 2) alpha_kernel(AlphaArgs<T, RP> A) {
   __shared__ double sm[kWarps * (kDotBatch + 1)];
   __shared__ double sh[kNcvMax];
   __shared__ double s_theta, s_s2;
+  __shared__ SpmvSmem<T> ssp;
+  __shared__ double sq[kNcvMax * (kDotBatch + 1)];
   AlphaCtrl* C = A.ctrl;
   const long long n = A.n;
   const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -262,6 +351,8 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
     C->nonfinite = 0;
     C->sig = 0ull;
     C->secant_sign = 1;
+    C->bytes = 0.0;
+    C->spmvs = 0;
   }
   {
     double ds = 0.0;
@@ -277,7 +368,10 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
   }
   if (!grid_barrier(&C->gs, [&] {
         reduce_partials(A.part, A.pw, gridDim.x, 1, sh);
-        if (threadIdx.x == 0) C->degree_scale = sh[0];
+        if (threadIdx.x == 0) {
+          C->degree_scale = sh[0];
+          C->bytes += (double)n * (8.0 + sizeof(T));
+        }
       })) return;
 
   if (mode == SA_START_SECANT && A.has_prev) {
@@ -286,7 +380,10 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
     block_store_partials<1>(v, A.part, A.pw, 0, sm);
     if (!grid_barrier(&C->gs, [&] {
           reduce_partials(A.part, A.pw, gridDim.x, 1, sh);
-          if (threadIdx.x == 0) C->secant_sign = (sh[0] < 0.0) ? -1 : 1;
+          if (threadIdx.x == 0) {
+            C->secant_sign = (sh[0] < 0.0) ? -1 : 1;
+            C->bytes += 2.0 * (double)n * sizeof(T);
+          }
         })) return;
   }
 
@@ -326,6 +423,8 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
           if (threadIdx.x == 0) {
             const int md = C->mode;
             const double nrm = sqrt(sh[0]);
+            const double nin = (md == SA_START_RANDOM) ? 0.0 : (md == SA_START_SECANT ? 2.0 : 1.0);
+            C->bytes += (double)n * sizeof(T) * (2.0 + nin) + (md == SA_START_DIAGONAL ? 8.0 * n : 0.0);
             C->action = ACT_NEXT;
             if (md == SA_START_DIAGONAL && nrm < kTinyNorm) {
               C->mode = SA_START_RANDOM;           // utils/predictors.py:22-25
@@ -354,31 +453,58 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
       const int j = vload(&C->j);
       const int pass2 = vload(&C->pass2);
       if (!pass2) {
-        // P1: V[j] = w * inv_b; w <- S V[j]
+        // P1: V[j] = w * inv_b; w <- S V[j]; partial sums of a_j = V[j] . w
         const T inv_b = (T)vload(&C->inv_b);
         T* Vj = A.V + (long long)j * A.ldv;
         const T trho = (T)rho;
-        spmv_dispatch<T, RP>(A.group, A.S, A.u, gwarp, nwarps, [&](long long r, T acc) {
-          const T wr = A.w[r];
-          Vj[r] = wr * inv_b;
-          A.w[r] = (trho * wr - A.sigma[r] * acc) * inv_b;
+        double pa[1] = {0.0};
+        spmv_items<T, RP>(A.S, A.u, gwarp, nwarps, ssp, [&](long long r, T acc) {
+          const T wr = __ldcg(A.w + r);
+          const T vr = wr * inv_b;
+          const T wn = (trho * wr - __ldcg(A.sigma + r) * acc) * inv_b;
+          Vj[r] = vr;
+          A.w[r] = wn;
+          pa[0] += (double)vr * (double)wn;
         });
-        if (!grid_barrier(&C->gs)) return;
+        block_store_partials<1>(pa, A.part, A.pw, 0, sm);
+        if (!grid_barrier(&C->gs, [&] {
+              reduce_partials(A.part, A.pw, gridDim.x, 1, sm);
+              if (threadIdx.x == 0) {
+                C->a[j] = sm[0];
+                C->bytes += A.spmv_bytes + (double)n * sizeof(T);
+                C->spmvs += 1;
+              }
+            })) return;
       }
-      // P2: h_k = V_k . w (k <= j), ww = w . w
-      for (int kb = 0; kb <= j; kb += kDotBatch) {
-        double acc[kDotBatch + 1];
+      // P2: three-term step w -= a_j V[j] + b_{j-1} V[j-1] (first pass only), then the
+      // reorthogonalisation coefficients h_k = V_k . w (k <= j) and ww = w . w. Removing the
+      // dominant components explicitly first keeps the single Gram-Schmidt pass stable.
+      {
+        const double a3 = pass2 ? 0.0 : vload(&C->a[j]);
+        const double b3 = (pass2 || j == 0) ? 0.0 : vload(&C->b[j - 1]);
+        const T* Vj = A.V + (long long)j * A.ldv;
+        const T* Vm = A.V + (long long)(j > 0 ? j - 1 : 0) * A.ldv;
+        for (int kb = 0; kb <= j; kb += kDotBatch) {
+          double acc[kDotBatch + 1];
 #pragma unroll
-        for (int q = 0; q <= kDotBatch; ++q) acc[q] = 0.0;
-        const int nk = (j + 1 - kb < kDotBatch) ? (j + 1 - kb) : kDotBatch;
-        for (long long i = gtid; i < n; i += nthreads) {
-          const double wi = (double)A.w[i];
+          for (int q = 0; q <= kDotBatch; ++q) acc[q] = 0.0;
+          const int nk = (j + 1 - kb < kDotBatch) ? (j + 1 - kb) : kDotBatch;
+          for (long long i = gtid; i < n; i += nthreads) {
+            double wi = (double)__ldcg(A.w + i);
+            if (kb == 0 && !pass2) {
+              wi -= a3 * (double)__ldcg(Vj + i);
+              if (j > 0) wi -= b3 * (double)__ldcg(Vm + i);
+              const T wt = (T)wi;
+              A.w[i] = wt;
+              wi = (double)wt;
+            }
 #pragma unroll
-          for (int q = 0; q < kDotBatch; ++q)
-            if (q < nk) acc[q] += (double)A.V[(long long)(kb + q) * A.ldv + i] * wi;
-          if (kb == 0) acc[kDotBatch] += wi * wi;
+            for (int q = 0; q < kDotBatch; ++q)
+              if (q < nk) acc[q] += (double)__ldcg(A.V + (long long)(kb + q) * A.ldv + i) * wi;
+            if (kb == 0) acc[kDotBatch] += wi * wi;
+          }
+          block_store_partials<kDotBatch + 1>(acc, A.part, A.pw, kb * 2, sm);
         }
-        block_store_partials<kDotBatch + 1>(acc, A.part, A.pw, kb * 2, sm);
       }
       if (!grid_barrier(&C->gs, [&] {
             // batch kb stored its 8 dots at cols [2kb, 2kb + 8) and ww (kb = 0) at col 8
@@ -390,8 +516,8 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
             }
             if (threadIdx.x == 0) {
               C->ww = sm[kDotBatch];
-              if (C->pass2) C->a[j] += sm[2 * ((j / kDotBatch) * kDotBatch) + (j % kDotBatch)];
-              else C->a[j] = sm[2 * ((j / kDotBatch) * kDotBatch) + (j % kDotBatch)];
+              C->a[j] += sm[2 * ((j / kDotBatch) * kDotBatch) + (j % kDotBatch)];
+              C->bytes += (double)n * sizeof(T) * (double)(j + 2 + (C->pass2 ? 0 : 3));
             }
           })) return;
       // P3: w -= sum_k h_k V_k ; u = sigma w ; ww2
@@ -401,8 +527,8 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
         double v[1] = {0.0};
         for (long long i = gtid; i < n; i += nthreads) {
           double corr = 0.0;
-          for (int k = 0; k <= j; ++k) corr += sh[k] * (double)A.V[(long long)k * A.ldv + i];
-          const T wi = (T)((double)A.w[i] - corr);
+          for (int k = 0; k <= j; ++k) corr += sh[k] * (double)__ldcg(A.V + (long long)k * A.ldv + i);
+          const T wi = (T)((double)__ldcg(A.w + i) - corr);
           A.w[i] = wi;
           A.u[i] = A.sigma[i] * wi;
           v[0] += (double)wi * (double)wi;
@@ -416,6 +542,7 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
             const double aj = C->a[j];
             if (threadIdx.x == 0) {
               C->action = ACT_NEXT;
+              C->bytes += (double)n * sizeof(T) * (double)(j + 5);
               if (!C->pass2) C->iters += 1;
               if (!isfinite(aj) || !isfinite(bj) || fabs(aj) > bound || bj > bound) {
                 C->status = SA_ERR_BREAKDOWN;   // models/spectral_annealing.py:85-120
@@ -458,11 +585,6 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
                   C->b[j] = bj;
                   C->action = ACT_DONE;
                 } else if (m >= ncv) {
-                  tridiag_eigvec(C->a, C->b, m, s_theta, C->s);
-                  const double coupling = bj * C->s[j];
-                  C->a[0] = s_theta;
-                  C->b[0] = coupling;
-                  C->inv_b = 1.0 / bj;
                   C->restarts += 1;
                   C->action = ACT_RESTART;
                 } else {
@@ -470,6 +592,11 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
                   C->inv_b = 1.0 / bj;
                   C->j = j + 1;
                 }
+              }
+              __syncthreads();
+              if (C->action == ACT_RESTART) {
+                const int kk = max(1, min(kDotBatch, ncv / 2));
+                implicit_restart(C, A.dense, A.dense + kNcvMax * kNcvMax, m, kk);
               }
             }
           })) return;
@@ -479,17 +606,66 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
       if (act == ACT_ERROR) return;
       if (act == ACT_REJECT) { restart_p0 = true; break; }
       if (act == ACT_RESTART) {
-        // V[0] <- V s (row-wise in place), keep w (the next vector) pending with inv_b
-        if (threadIdx.x <= j) sh[threadIdx.x] = vload(&C->s[threadIdx.x]);
-        __syncthreads();
-        for (long long i = gtid; i < n; i += nthreads) {
-          double y = 0.0;
-          for (int k = 0; k <= j; ++k) y += sh[k] * (double)A.V[(long long)k * A.ldv + i];
-          A.V[i] = (T)y;
+        // kept basis V[0..kk) <- V Q[:, 0..kk) and the new residual
+        // f = V Q[:, kk] T+[kk][kk-1] + w Q[m-1][kk-1], row by row in place (all m inputs of a row
+        // are read before its kk outputs are written)
+        const int m = j + 1;
+        const int kk = vload(&C->irl_k);
+        const double beta_hat = vload(&C->irl_beta), sig_q = vload(&C->irl_sigma);
+        const double* Qd = A.dense + kNcvMax * kNcvMax;
+        for (int idx = threadIdx.x; idx < m * (kk + 1); idx += blockDim.x) {
+          const int r = idx / (kk + 1), c = idx % (kk + 1);
+          sq[idx] = vload(Qd + r * m + c);
         }
+        __syncthreads();
+        double v[1] = {0.0};
+        for (long long i = gtid; i < n; i += nthreads) {
+          double y[kDotBatch + 1];
+#pragma unroll
+          for (int c = 0; c <= kDotBatch; ++c) y[c] = 0.0;
+          for (int r = 0; r < m; ++r) {
+            const double vr = (double)A.V[(long long)r * A.ldv + i];
+#pragma unroll
+            for (int c = 0; c <= kDotBatch; ++c)
+              if (c <= kk) y[c] += vr * sq[r * (kk + 1) + c];
+          }
+#pragma unroll
+          for (int c = 0; c < kDotBatch; ++c)
+            if (c < kk) A.V[(long long)c * A.ldv + i] = (T)y[c];
+          double yk = 0.0;
+#pragma unroll
+          for (int c = 0; c <= kDotBatch; ++c)
+            if (c == kk) yk = y[c];
+          const T f = (T)(yk * beta_hat + (double)A.w[i] * sig_q);
+          A.w[i] = f;
+          A.u[i] = A.sigma[i] * f;
+          v[0] += (double)f * (double)f;
+        }
+        block_store_partials<1>(v, A.part, A.pw, 0, sm);
         if (!grid_barrier(&C->gs, [&] {
-              if (threadIdx.x == 0) { C->j = 1; C->pass2 = 0; }
+              reduce_partials(A.part, A.pw, gridDim.x, 1, sm);
+              if (threadIdx.x == 0) {
+                const double nf = sqrt(sm[0]);
+                C->pass2 = 0;
+                C->bytes += (double)n * sizeof(T) * (double)(m + kk + 3);
+                if (!(nf > 1e-14 * bound) || !isfinite(nf)) {
+                  // the kept basis spans an invariant subspace: finish with its Ritz vector
+                  const double th = kth_eig(C->a, C->b, kk, 0);
+                  C->theta = th;
+                  tridiag_eigvec(C->a, C->b, kk, th, C->s);
+                  C->j = kk - 1;
+                  C->res_est = 0.0;
+                  C->status = SA_OK;
+                  C->action = ACT_DONE;
+                } else {
+                  C->b[kk - 1] = nf;
+                  C->inv_b = 1.0 / nf;
+                  C->j = kk;
+                  C->action = ACT_NEXT;
+                }
+              }
             })) return;
+        if (vload(&C->action) == ACT_DONE) break;
         continue;
       }
       break;   // ACT_DONE
@@ -508,7 +684,7 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
     const bool align = P.align && A.has_last;
     for (long long i = gtid; i < n; i += nthreads) {
       double y = 0.0;
-      for (int k = 0; k <= jf; ++k) y += sh[k] * (double)A.V[(long long)k * A.ldv + i];
+      for (int k = 0; k <= jf; ++k) y += sh[k] * (double)__ldcg(A.V + (long long)k * A.ldv + i);
       const T yt = (T)y;
       if (!isfinite((double)yt)) bad = 1;
       A.yout[i] = yt;
@@ -526,6 +702,7 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
           const bool align = P.align && A.has_last;
           C->nrm_y = nrm;
           C->align_dot = align ? sh[1] : 0.0;
+          C->bytes += (double)n * sizeof(T) * (double)(jf + 3 + (align ? 1 : 0));
           const double sg = (align && sh[1] < 0.0) ? -1.0 : 1.0;
           C->scale = (nrm > 0.0) ? sg / nrm : sg;
         }
@@ -538,9 +715,10 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
     double v[1] = {0.0};
     if (P.residual_check) {
       const T trho = (T)rho;
-      spmv_dispatch<T, RP>(A.group, A.S, A.u, gwarp, nwarps, [&](long long r, T acc) {
-        const double yr = (double)A.yout[r];
-        const double sy = (double)(trho * A.yout[r] - A.sigma[r] * acc);
+      spmv_items<T, RP>(A.S, A.u, gwarp, nwarps, ssp, [&](long long r, T acc) {
+        const T yt = __ldcg(A.yout + r);
+        const double yr = (double)yt;
+        const double sy = (double)(trho * yt - __ldcg(A.sigma + r) * acc);
         const double rr = sy - theta * yr;
         v[0] += rr * rr;
       });
@@ -567,7 +745,12 @@ __global__ void __launch_bounds__(kThreads) alpha_kernel(AlphaArgs<T, RP> A) {
   }
   if (!grid_barrier(&C->gs, [&] {
         reduce_partials(A.part, A.pw, gridDim.x, 1, sh);
-        if (threadIdx.x == 0) C->rr = sh[0];
+        if (threadIdx.x == 0) {
+          C->rr = sh[0];
+          if (P.residual_check) { C->bytes += A.spmv_bytes; C->spmvs += 1; }
+          if (P.round) C->bytes += (double)n * sizeof(T) + (double)n / 8.0;
+          C->bytes += 2.0 * (double)n * sizeof(T);   // F3
+        }
       })) return;
   // F3: y <- scale * y (aligned, unit norm)
   {
@@ -611,9 +794,12 @@ static int launch_alpha(sa_handle* h, const sa_alpha_params* p) {
   A.half_log2_c = 0.5 * std::log2(h->c);
   A.sqrt_c = std::sqrt(h->c);
   A.group = h->group;
+  A.dense = h->dense;
+  A.spmv_bytes = (double)h->nnz * (4.0 + sizeof(T)) + (double)(h->n + 1) * sizeof(RP) + 3.0 * (double)h->n * sizeof(T);
   void* args[] = {&A};
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)alpha_kernel<T, RP>, dim3(h->blocks),
                                               dim3(kThreads), args, 0, h->stream);
+  count_launches(1);
   return e == cudaSuccess ? SA_OK : SA_ERR_CUDA;
 }
 

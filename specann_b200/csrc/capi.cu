@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -10,7 +11,11 @@
 #include "handle.cuh"
 #include "spmv.cuh"
 
+#include <atomic>
+
 namespace sa {
+static std::atomic<unsigned long long> g_launches{0};
+void count_launches(int k) { g_launches.fetch_add((unsigned long long)k, std::memory_order_relaxed); }
 int alpha_solve_impl(sa_handle* h, const sa_alpha_params* p);
 const void* alpha_kernel_for(int prec, int rp64);
 const void* ls_kernel_for(int prec, int rp64, int integer);
@@ -31,7 +36,7 @@ namespace {
 
 struct Carve {
   size_t sigma, ld, deg, V, w, u, y0, y1, y2, items, mc_base, mc_count, long_part, blk_part, actrl, red,
-      cand, refined, scratch, total;
+      cand, refined, scratch, dense, total;
 };
 
 constexpr int kMaxBlocks = 1024;
@@ -44,7 +49,7 @@ Carve carve(long long n, long long nnz, int prec, int ncv_max, int max_cand) {
   Layout L;
   Carve c;
   c.sigma = L.off(T * n);
-  c.ld = L.off(4 * n);
+  c.ld = L.off(8 * n);
   c.deg = L.off(8 * n);
   c.V = L.off(T * (size_t)ldv * ncv_max);
   c.w = L.off(T * n);
@@ -62,6 +67,7 @@ Carve carve(long long n, long long nnz, int prec, int ncv_max, int max_cand) {
   c.cand = L.off(4 * (size_t)W * max_cand);
   c.refined = L.off(4 * (size_t)W * max_cand);
   c.scratch = L.off(4 * (size_t)W);
+  c.dense = L.off(8 * 2 * (size_t)kNcvMax * kNcvMax);
   c.total = L.total;
   return c;
 }
@@ -71,21 +77,23 @@ Carve carve(long long n, long long nnz, int prec, int ncv_max, int max_cand) {
 struct DegRed {
   unsigned long long dmax_bits, dmin_bits;
   int nonint;
-  int pad;
+  int badcol;   // a column index outside [0, n)
 };
 
 template <typename T, typename RP>
-__global__ void degree_kernel(const RP* rp, const T* val, long long n, double* deg, DegRed* red) {
+__global__ void degree_kernel(const RP* rp, const int* col, const T* val, long long n, double* deg, DegRed* red) {
   __shared__ unsigned long long s_max, s_min;
   __shared__ int s_nonint;
   if (threadIdx.x == 0) { s_max = 0ull; s_min = ~0ull; s_nonint = 0; }
   __syncthreads();
   unsigned long long lmax = 0ull, lmin = ~0ull;
-  int nonint = 0;
+  int nonint = 0, badcol = 0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const long long b = rp_load(rp, i), e = rp_load(rp, i + 1);
     double s = 0.0;
     for (long long p = b; p < e; ++p) {
+      const int cidx = __ldg(col + p);
+      if (cidx < 0 || (long long)cidx >= n) badcol = 1;
       const double v = (double)__ldg(val + p);
       s += fabs(v);
       if (!(v == rint(v)) || fabs(v) > 16777216.0) nonint = 1;
@@ -98,6 +106,7 @@ __global__ void degree_kernel(const RP* rp, const T* val, long long n, double* d
   atomicMax(&s_max, lmax);
   atomicMin(&s_min, lmin);
   if (nonint) s_nonint = 1;
+  if (badcol) atomicOr(&red->badcol, 1);
   __syncthreads();
   if (threadIdx.x == 0) {
     atomicMax(&red->dmax_bits, s_max);
@@ -106,16 +115,16 @@ __global__ void degree_kernel(const RP* rp, const T* val, long long n, double* d
   }
 }
 
-__global__ void logdeg_kernel(const double* deg, long long n, double c, float* ld) {
+__global__ void logdeg_kernel(const double* deg, long long n, double c, double* ld) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const double d = deg[i] / c;
-    ld[i] = d > 0.0 ? (float)log2(d) : -INFINITY;
+    ld[i] = d > 0.0 ? log2(d) : -INFINITY;
   }
 }
 
 // sigma = D^{-1/2} / sqrt(c) for this alpha and u = sigma * x.
 template <typename T>
-__global__ void scale_kernel(const float* ld, long long n, double alpha, double half_log2_c, const T* x,
+__global__ void scale_kernel(const double* ld, long long n, double alpha, double half_log2_c, const T* x,
                              T* sigma, T* u) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const double logD = (alpha == 0.0) ? 0.0 : alpha * (double)ld[i];
@@ -127,11 +136,12 @@ __global__ void scale_kernel(const float* ld, long long n, double alpha, double 
 }
 
 template <typename T, typename RP>
-__global__ void __launch_bounds__(kThreads) spmv_kernel(SpmvArgs<T, RP> S, int group, const T* u, const T* x,
+__global__ void __launch_bounds__(kThreads, 3) spmv_kernel(SpmvArgs<T, RP> S, int group, const T* u, const T* x,
                                                          const T* sigma, T rho, T* y) {
+  __shared__ SpmvSmem<T> ssp;
   const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nthreads = (long long)gridDim.x * blockDim.x;
-  spmv_dispatch<T, RP>(group, S, u, gtid >> 5, nthreads >> 5, [&](long long r, T acc) {
+  spmv_items<T, RP, true>(S, u, gtid >> 5, nthreads >> 5, ssp, [&](long long r, T acc) {
     y[r] = rho * x[r] - sigma[r] * acc;
   });
 }
@@ -160,7 +170,7 @@ __device__ __forceinline__ unsigned long long word_mix_host(long long widx, unsi
 
 template <typename T>
 __global__ void round_kernel(const T* y, long long n, double alpha, double half_log2_c, double sqrt_c,
-                             const float* ld, T scale, T* yout, uint32_t* bits, unsigned long long* sig) {
+                             const double* ld, T scale, T* yout, uint32_t* bits, unsigned long long* sig) {
   const long long nr = (n + 31) & ~31ll;
   unsigned long long hs = 0ull;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += (long long)gridDim.x * blockDim.x) {
@@ -228,12 +238,13 @@ void build_items(const std::vector<long long>& rp, long long n, std::vector<Work
         for (long long c = 0; c < nch; ++c) items.push_back(WorkItem{-(r + 1), (int)c, z});
       }
     } else {
+      if (seg_begin >= 0 && seg_elems + d > kSegMax) flush(r);
       if (seg_begin < 0) seg_begin = r;
       ++seg_rows;
       seg_elems += d;
       ++short_rows;
       short_elems += d;
-      if (seg_rows >= kSegRows || seg_elems > kSegElems) flush(r + 1);
+      if (seg_rows >= kSegRows) flush(r + 1);
     }
   }
   flush(n);
@@ -246,6 +257,8 @@ void build_items(const std::vector<long long>& rp, long long n, std::vector<Work
 extern "C" {
 
 const char* sa_version(void) { return "specann_b200 0.1 (sm_100a)"; }
+
+uint64_t sa_kernel_launches(void) { return (uint64_t)g_launches.load(std::memory_order_relaxed); }
 
 int sa_workspace_size(int64_t n, int64_t nnz, int32_t rowptr64, int32_t precision, int32_t ncv_max,
                       int32_t max_candidates, size_t* bytes) {
@@ -281,7 +294,7 @@ int sa_create(sa_handle** out, int64_t n, int64_t nnz, int32_t rowptr64, int32_t
   h->ldv = (n + 63) & ~63ll;
   h->W = (n + 31) / 32;
   h->sigma = h->ws + c.sigma;
-  h->ld = (float*)(h->ws + c.ld);
+  h->ld = (double*)(h->ws + c.ld);
   h->deg = (double*)(h->ws + c.deg);
   h->V = h->ws + c.V;
   h->w = h->ws + c.w;
@@ -303,6 +316,7 @@ int sa_create(sa_handle** out, int64_t n, int64_t nnz, int32_t rowptr64, int32_t
   h->cand = (uint32_t*)(h->ws + c.cand);
   h->refined = (uint32_t*)(h->ws + c.refined);
   h->scratch = (uint32_t*)(h->ws + c.scratch);
+  h->dense = (double*)(h->ws + c.dense);
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { delete h; return SA_ERR_CUDA; }
   if (cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) { delete h; return SA_ERR_CUDA; }
@@ -337,21 +351,7 @@ int sa_set_matrix(sa_handle* h, const void* rowptr, const int32_t* col, const vo
   h->rowptr = rowptr;
   h->col = col;
   h->val = val;
-  DegRed init{0ull, ~0ull, 0, 0};
-  DegRed* dred = (DegRed*)h->red;
-  SA_CUDA(cudaMemcpyAsync(dred, &init, sizeof(DegRed), cudaMemcpyHostToDevice, h->stream));
-  const int g = grid_for(h->n, 256, h->sm_count);
-  if (h->prec == 32) {
-    if (h->rp64) degree_kernel<float, long long><<<g, 256, 0, h->stream>>>((const long long*)rowptr, (const float*)val, h->n, h->deg, dred);
-    else degree_kernel<float, int><<<g, 256, 0, h->stream>>>((const int*)rowptr, (const float*)val, h->n, h->deg, dred);
-  } else {
-    if (h->rp64) degree_kernel<double, long long><<<g, 256, 0, h->stream>>>((const long long*)rowptr, (const double*)val, h->n, h->deg, dred);
-    else degree_kernel<double, int><<<g, 256, 0, h->stream>>>((const int*)rowptr, (const double*)val, h->n, h->deg, dred);
-  }
-  SA_CUDA(cudaGetLastError());
-  DegRed r;
-  SA_CUDA(cudaMemcpyAsync(&r, dred, sizeof(DegRed), cudaMemcpyDeviceToHost, h->stream));
-  // row pointers to the host for the work list
+  // row pointers to the host first: validated before any kernel reads through them
   std::vector<long long> rp(h->n + 1);
   if (h->rp64) {
     SA_CUDA(cudaMemcpyAsync(rp.data(), rowptr, sizeof(long long) * (h->n + 1), cudaMemcpyDeviceToHost, h->stream));
@@ -365,6 +365,24 @@ int sa_set_matrix(sa_handle* h, const void* rowptr, const int32_t* col, const vo
   if (rp[0] != 0 || rp[h->n] != h->nnz) return SA_ERR_INVALID_ARG;
   for (long long i = 0; i < h->n; ++i)
     if (rp[i + 1] < rp[i]) return SA_ERR_INVALID_ARG;
+  DegRed init{0ull, ~0ull, 0, 0};
+  DegRed* dred = (DegRed*)h->red;
+  SA_CUDA(cudaMemcpyAsync(dred, &init, sizeof(DegRed), cudaMemcpyHostToDevice, h->stream));
+  const int g = grid_for(h->n, 256, h->sm_count);
+  if (h->prec == 32) {
+    if (h->rp64) degree_kernel<float, long long><<<g, 256, 0, h->stream>>>((const long long*)rowptr, col, (const float*)val, h->n, h->deg, dred);
+    else degree_kernel<float, int><<<g, 256, 0, h->stream>>>((const int*)rowptr, col, (const float*)val, h->n, h->deg, dred);
+    count_launches(1);
+  } else {
+    if (h->rp64) degree_kernel<double, long long><<<g, 256, 0, h->stream>>>((const long long*)rowptr, col, (const double*)val, h->n, h->deg, dred);
+    else degree_kernel<double, int><<<g, 256, 0, h->stream>>>((const int*)rowptr, col, (const double*)val, h->n, h->deg, dred);
+    count_launches(1);
+  }
+  SA_CUDA(cudaGetLastError());
+  DegRed r;
+  SA_CUDA(cudaMemcpyAsync(&r, dred, sizeof(DegRed), cudaMemcpyDeviceToHost, h->stream));
+  SA_CUDA(cudaStreamSynchronize(h->stream));
+  if (r.badcol) return SA_ERR_INVALID_ARG;
   double dmax, dmin;
   memcpy(&dmax, &r.dmax_bits, 8);
   memcpy(&dmin, &r.dmin_bits, 8);
@@ -374,6 +392,7 @@ int sa_set_matrix(sa_handle* h, const void* rowptr, const int32_t* col, const vo
   h->integer_J = (r.nonint == 0 && dmax < 1073741824.0) ? 1 : 0;
   if (!(dmax > 0.0) || !std::isfinite(dmax)) return SA_ERR_INVALID_ARG;
   logdeg_kernel<<<g, 256, 0, h->stream>>>(h->deg, h->n, h->c, h->ld);
+  count_launches(1);
   SA_CUDA(cudaGetLastError());
   std::vector<WorkItem> items;
   std::vector<long long> mc_base;
@@ -408,26 +427,33 @@ int sa_spmv_scaled(sa_handle* h, double alpha, double rho, const void* x, void* 
   if (!h || !h->bound || !x || !y) return SA_ERR_INVALID_ARG;
   const int g = grid_for(h->n, 256, h->sm_count);
   const double hl = 0.5 * std::log2(h->c);
-  const int gs = h->sm_count * 4;
+  const int gs = h->sm_count * 3;
+  if (h->n_mc) SA_CUDA(cudaMemsetAsync(h->mc_count, 0, 4 * h->n_mc, h->stream));
   if (h->prec == 32) {
     scale_kernel<float><<<g, 256, 0, h->stream>>>(h->ld, h->n, alpha, hl, (const float*)x, (float*)h->sigma, (float*)h->u);
+    count_launches(1);
     SpmvArgs<float, int> S32;
     SpmvArgs<float, long long> S64;
     if (h->rp64) {
       S64 = SpmvArgs<float, long long>{(const long long*)h->rowptr, h->col, (const float*)h->val, h->items, h->n_items, h->mc_base, h->mc_count, (float*)h->long_part};
       spmv_kernel<float, long long><<<gs, kThreads, 0, h->stream>>>(S64, h->group, (const float*)h->u, (const float*)x, (const float*)h->sigma, (float)rho, (float*)y);
+      count_launches(1);
     } else {
       S32 = SpmvArgs<float, int>{(const int*)h->rowptr, h->col, (const float*)h->val, h->items, h->n_items, h->mc_base, h->mc_count, (float*)h->long_part};
       spmv_kernel<float, int><<<gs, kThreads, 0, h->stream>>>(S32, h->group, (const float*)h->u, (const float*)x, (const float*)h->sigma, (float)rho, (float*)y);
+      count_launches(1);
     }
   } else {
     scale_kernel<double><<<g, 256, 0, h->stream>>>(h->ld, h->n, alpha, hl, (const double*)x, (double*)h->sigma, (double*)h->u);
+    count_launches(1);
     if (h->rp64) {
       SpmvArgs<double, long long> S{(const long long*)h->rowptr, h->col, (const double*)h->val, h->items, h->n_items, h->mc_base, h->mc_count, (double*)h->long_part};
       spmv_kernel<double, long long><<<gs, kThreads, 0, h->stream>>>(S, h->group, (const double*)h->u, (const double*)x, (const double*)h->sigma, rho, (double*)y);
+      count_launches(1);
     } else {
       SpmvArgs<double, int> S{(const int*)h->rowptr, h->col, (const double*)h->val, h->items, h->n_items, h->mc_base, h->mc_count, (double*)h->long_part};
       spmv_kernel<double, int><<<gs, kThreads, 0, h->stream>>>(S, h->group, (const double*)h->u, (const double*)x, (const double*)h->sigma, rho, (double*)y);
+      count_launches(1);
     }
   }
   SA_CUDA(cudaGetLastError());
@@ -465,6 +491,14 @@ int sa_alpha_solve(sa_handle* h, const sa_alpha_params* p, sa_alpha_record* rec)
   rec->signature = ctl.sig;
   rec->nonfinite = ctl.nonfinite;
   rec->basis_used = ctl.j + 1;
+  rec->spmv_count = ctl.spmvs;
+  rec->alg_bytes = ctl.bytes;
+  if (rec->status != SA_OK && std::getenv("SPECANN_DEBUG")) {
+    std::fprintf(stderr, "[specann] alpha_solve status %d: j=%d iters=%d restarts=%d action=%d theta=%.17g ww=%.6g inv_b=%.6g\n",
+                 rec->status, ctl.j, ctl.iters, ctl.restarts, ctl.action, ctl.theta, ctl.ww, ctl.inv_b);
+    for (int i = 0; i <= ctl.j && i < kNcvMax; ++i)
+      std::fprintf(stderr, "  a[%d]=%.17g b[%d]=%.17g h[%d]=%.17g\n", i, ctl.a[i], i, ctl.b[i], i, ctl.h[i]);
+  }
   return SA_OK;
 }
 
@@ -501,6 +535,7 @@ int sa_round_vector(sa_handle* h, double alpha, const void* y, int32_t align, ui
   const int use_last = (align && h->has_last) ? 1 : 0;
   if (h->prec == 32) norm_dot_kernel<float><<<g, 256, 0, h->stream>>>((const float*)y, (const float*)h->yv[h->iy_last], h->n, use_last, part);
   else norm_dot_kernel<double><<<g, 256, 0, h->stream>>>((const double*)y, (const double*)h->yv[h->iy_last], h->n, use_last, part);
+  count_launches(1);
   SA_CUDA(cudaGetLastError());
   std::vector<double> hp(2 * g);
   SA_CUDA(cudaMemcpyAsync(hp.data(), part, sizeof(double) * 2 * g, cudaMemcpyDeviceToHost, h->stream));
@@ -515,6 +550,7 @@ int sa_round_vector(sa_handle* h, double alpha, const void* y, int32_t align, ui
   const double hl = 0.5 * std::log2(h->c), sc = std::sqrt(h->c);
   if (h->prec == 32) round_kernel<float><<<g, 256, 0, h->stream>>>((const float*)y, h->n, alpha, hl, sc, h->ld, (float)scale, (float*)h->yv[h->iy_out], h->scratch, sig);
   else round_kernel<double><<<g, 256, 0, h->stream>>>((const double*)y, h->n, alpha, hl, sc, h->ld, scale, (double*)h->yv[h->iy_out], h->scratch, sig);
+  count_launches(1);
   SA_CUDA(cudaGetLastError());
   unsigned long long s = 0;
   SA_CUDA(cudaMemcpyAsync(&s, sig, 8, cudaMemcpyDeviceToHost, h->stream));
@@ -534,6 +570,7 @@ int sa_candidate_equal(sa_handle* h, int32_t slot, int32_t* equal) {
   int* flag = (int*)h->red;
   SA_CUDA(cudaMemsetAsync(flag, 0, 4, h->stream));
   compare_kernel<<<grid_for(h->W, 256, h->sm_count), 256, 0, h->stream>>>(h->cand + (size_t)slot * h->W, h->scratch, h->W, flag);
+  count_launches(1);
   SA_CUDA(cudaGetLastError());
   int d = 0;
   SA_CUDA(cudaMemcpyAsync(&d, flag, 4, cudaMemcpyDeviceToHost, h->stream));
@@ -559,6 +596,7 @@ int sa_candidate_unpack(sa_handle* h, int32_t slot, int32_t refined, int8_t* spi
   if (!h || !spins_device || slot < -1 || slot >= h->max_cand) return SA_ERR_INVALID_ARG;
   const uint32_t* src = slot < 0 ? h->scratch : (refined ? h->refined : h->cand) + (size_t)slot * h->W;
   unpack_kernel<<<grid_for(h->n, 256, h->sm_count), 256, 0, h->stream>>>(src, h->n, spins_device);
+  count_launches(1);
   SA_CUDA(cudaGetLastError());
   return SA_OK;
 }
@@ -572,7 +610,7 @@ int sa_ls_workspace_size(sa_handle* h, int32_t k, size_t* bytes) {
 int sa_local_search(sa_handle* h, const sa_ls_params* p, void* ls_workspace, size_t ls_bytes,
                     double* energies_before, double* energies_after, sa_ls_result* result) {
   if (!h || !h->bound || !p || !ls_workspace || p->k < 1 || p->first_slot < 0 ||
-      p->first_slot + p->k > h->max_cand || p->max_iterations < 0 ||
+      p->first_slot + p->k > h->max_cand || p->max_iterations < 0 || p->semantics < 0 || p->semantics > 1 ||
       p->num_rounds < 0 || p->final_sweep_iters < 0)
     return SA_ERR_INVALID_ARG;
   if (((uintptr_t)ls_workspace) & 255) return SA_ERR_INVALID_ARG;

@@ -10,7 +10,10 @@ namespace sa {
 constexpr int kThreads = 512;             // threads per CTA of the persistent kernels
 constexpr int kWarps = kThreads / 32;
 constexpr int kShortMax = 64;             // rows with at most this many entries are "short"
-constexpr int kChunk = 1024;              // entries per chunk of a long row
+constexpr int kChunk = 256;               // entries per chunk of a long row
+constexpr int kSegMax = 256;              // entries per short segment at most (= one warp tile)
+constexpr int kSegRows = 64;              // rows per short segment at most
+constexpr int kTileIt = kSegMax / 32;     // entries per lane of a tile
 constexpr int kNcvMax = 64;               // largest Lanczos basis
 constexpr int kDotBatch = 8;              // basis vectors per register batch in the dot phase
 constexpr unsigned long long kSpinLimit = 1ull << 25;   // ~2 s of 64 ns sleeps

@@ -38,6 +38,11 @@ struct AlphaCtrl {
   double degree_scale;
   double align_dot;
   double res_est;
+  double bytes;             // algorithmic DRAM bytes of this launch
+  int spmvs;                // fused SpMVs run by this launch
+  int irl_k;                // basis vectors kept by the last implicit restart
+  double irl_beta;          // T+[k][k-1] of the last implicit restart
+  double irl_sigma;         // Q[m-1][k-1] of the last implicit restart
 };
 
 // Control block of the local-search kernel.
@@ -51,6 +56,7 @@ struct LsCtrl {
   long long stream;         // selection stream of the current pass
   long long m;              // nodes selected in the current pass
   long long wl_count;       // work-list entries of the current pass
+  long long wq_count;       // wanting nodes of the current pass (priority passes)
   long long total_flips;
   unsigned int active[4];   // candidates that have not yet had a pass without a flip
   long long counts[128];    // flips per candidate in the current pass
@@ -65,12 +71,12 @@ struct Layout {
   }
 };
 
-// Upper bounds of the SpMV work list for a matrix of n rows and nnz entries.
-constexpr int kSegRows = 96;     // rows per short segment at most
-constexpr int kSegElems = 512;   // entries per short segment (a segment is closed once it has more)
-
+// Upper bound of the SpMV work list for a matrix of n rows and nnz entries: a short segment is
+// closed when it has kSegRows rows or the next row would take it past kSegMax entries (so it
+// holds more than kSegMax - kShortMax entries, or kSegRows rows, unless a long row or the end
+// follows it); a long row gives at most nnz_row / kChunk + 1 chunks.
 inline long long max_items(long long n, long long nnz) {
-  return n / kSegRows + nnz / kSegElems + 2 * (nnz / (kShortMax + 1)) + nnz / kChunk + 8;
+  return n / kSegRows + nnz / (kSegMax - kShortMax) + 2 * (nnz / (kShortMax + 1)) + nnz / kChunk + 8;
 }
 inline long long max_multichunk_rows(long long nnz) { return nnz / (kChunk + 1) + 1; }
 inline long long max_long_partials(long long nnz) { return nnz / kChunk + max_multichunk_rows(nnz) + 1; }
@@ -93,7 +99,7 @@ struct sa_handle {
   // workspace carve-out
   long long ldv = 0;            // leading dimension of basis vectors (n rounded up to 64)
   void* sigma = nullptr;        // D^{-1/2} / sqrt(c) for the current alpha (T)
-  float* ld = nullptr;          // log2 d (float)
+  double* ld = nullptr;         // log2 d (double)
   double* deg = nullptr;        // absolute degrees (double)
   void* V = nullptr;            // Lanczos basis, ncv_max x ldv (T)
   void* w = nullptr;
@@ -111,6 +117,7 @@ struct sa_handle {
   double* blk_part = nullptr;
   int blk_part_width = 0;
   sa::AlphaCtrl* actrl = nullptr;
+  double* dense = nullptr;      // implicit-restart scratch: dense T and Q (2 x kNcvMax^2 doubles)
   double* red = nullptr;        // small reduction scratch (set-up kernels)
   uint32_t* cand = nullptr;     // candidate store, max_cand x W
   uint32_t* refined = nullptr;  // refined candidates, max_cand x W

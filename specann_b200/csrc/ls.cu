@@ -1,6 +1,11 @@
 // Batched single-flip local search over all distinct candidates as one persistent cooperative
 // kernel, with a cache of the local fields h_ic = sum_j J_ij s_cj and snapshot passes.
 //
+// Pass semantics (both decided from the pass-start state; bit-exact with oracle/specann_oracle.py):
+//   priority (default): a wanting node flips unless a wanting neighbour has a lower rank in the
+//     pass's permutation, so the flips form an independent set and every flip lowers the energy
+//     by its gain (phases D1: wanting masks and ranks, D2: blocking check, U);
+//   snapshot: every wanting node flips (phases D, U).
 // Layout (node-major, so one read of a CSR row serves every candidate):
 //   sb[i * kw + t]     bit c of word t: spin of candidate 32 t + c at node i is +1
 //   h[i * kp + c]      local field of node i in candidate c (int32 for integer couplings, which
@@ -9,7 +14,9 @@
 // A pass: (D) every selected node decides for every candidate from the pass-start state, flips
 // its own spin bits and appends (node, chunk) entries to a work list; (U) one warp per entry
 // scatters the field changes 2 J_ij s_i(new) to the neighbours of the chunk for the flipped
-// candidates (integer atomics: exact and order-independent). The last CTA at each barrier runs
+// candidates (integer atomics: exact and order-independent). Arrays that other CTAs change during
+// the kernel (h, sb, flipm, the work list) are read with ld.global.cg: the per-SM L1 is not
+// coherent with their writes. The last CTA at each barrier runs
 // the stopping rules of flip_refinement / gpu_final_sweep (models/spectral_annealing.py:983-1112).
 #include <cmath>
 #include <cstring>
@@ -20,6 +27,8 @@
 #include "spmv.cuh"
 
 namespace sa {
+
+void count_launches(int k);
 
 template <typename GT>
 struct EAccOf { using type = typename std::conditional<std::is_same<GT, int>::value, long long, double>::type; };
@@ -39,6 +48,10 @@ struct LsArgs {
   uint32_t* flipm;
   long long* wl;
   long long wl_cap;
+  uint32_t* wm;          // wanting masks of the pass (priority passes), n x kw
+  int* prio;             // rank of the node in the pass's permutation (INT_MAX if not selected)
+  int* wq;               // wanting nodes of the pass
+  int priority;          // 1: priority passes, 0: snapshot passes
   LsCtrl* ctrl;
   EAccPtr ebefore;      // kp sums of s_i h_i (energy = -sum / 2): int64 or double
   EAccPtr eafter;
@@ -108,8 +121,8 @@ __device__ void energy_phase(const LsArgs<VT, RP, GT>& A, EAcc<GT>* out, EAcc<GT
     for (long long base = gwarp * ne; base < A.n; base += nwarps * ne) {
       const long long i = base + slot;
       if (i < A.n) {
-        const uint32_t word = A.sb[i * A.kw + t];
-        const GT hv = A.h[i * A.kp + 32 * t + c];
+        const uint32_t word = __ldcg(A.sb + i * A.kw + t);
+        const GT hv = __ldcg(A.h + i * A.kp + 32 * t + c);
         acc += ((word >> c) & 1u) ? (E)hv : -(E)hv;
       }
     }
@@ -136,6 +149,7 @@ __global__ void __launch_bounds__(kThreads) ls_kernel(LsArgs<VT, RP, GT> A) {
   // ---- L0: candidate-major packed spins -> node-major bits; zero the fields -----------------
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     C->it = 0; C->round = 0; C->sub = 0; C->final_passes = 0; C->total_flips = 0; C->wl_count = 0;
+    C->wq_count = 0;
     for (int q = 0; q < 4; ++q) C->active[q] = 0u;
     for (int q = 0; q < A.k; ++q) C->active[q >> 5] |= 1u << (q & 31);
     for (int q = 0; q < 128; ++q) C->counts[q] = 0;
@@ -195,11 +209,22 @@ __global__ void __launch_bounds__(kThreads) ls_kernel(LsArgs<VT, RP, GT> A) {
     const SelKeys keys = make_sel_keys(A.p.seed, stream, n);
     for (int q = threadIdx.x; q < 128; q += blockDim.x) s_cnt[q] = 0;
     __syncthreads();
-    // D: decide, flip own bits, append work-list entries
+    // D1: every selected node decides for every candidate from the pass-start state. Snapshot
+    // passes flip the wanting pairs here; priority passes record the wanting masks and ranks.
     int cnt[4] = {0, 0, 0, 0};
     for (long long tile = gwarp * 32; tile < n; tile += nwarps * 32) {
       bool selb = false;
-      if (tile + lane < n) selb = all_sel || sel_rank(tile + lane, keys, n) < m;
+      int rk = 0x7fffffff;
+      if (tile + lane < n) {
+        if (all_sel && !A.priority) {
+          selb = true;
+        } else {
+          const long long r = sel_rank(tile + lane, keys, n);
+          selb = r < m;
+          rk = (int)r;
+        }
+        if (A.priority) A.prio[tile + lane] = selb ? rk : 0x7fffffff;
+      }
       const uint32_t selmask = __ballot_sync(0xffffffffu, selb);
       for (int sub = 0; sub < 32; sub += ne) {
         const long long i = tile + sub + slot;
@@ -209,21 +234,29 @@ __global__ void __launch_bounds__(kThreads) ls_kernel(LsArgs<VT, RP, GT> A) {
           bool f = false;
           uint32_t word = 0u;
           if (valid) {
-            word = A.sb[i * A.kw + t];
-            const GT hv = A.h[i * A.kp + 32 * t + c];
+            word = __ldcg(A.sb + i * A.kw + t);
+            const GT hv = __ldcg(A.h + i * A.kp + 32 * t + c);
             const bool sp = (word >> c) & 1u;
             f = (32 * t + c < A.k) && (sp ? (hv < GT(0)) : (hv > GT(0)));
           }
           const uint32_t bal = __ballot_sync(0xffffffffu, f);
           const uint32_t bits = (cp == 32) ? bal : ((bal >> (slot * cp)) & ((1u << cp) - 1u));
           fl[t] = bits;
-          cnt[t] += f ? 1 : 0;
-          if (c == 0 && bits) A.sb[i * A.kw + t] = word ^ bits;
+          if (!A.priority) {
+            cnt[t] += f ? 1 : 0;
+            if (c == 0 && bits) A.sb[i * A.kw + t] = word ^ bits;
+          }
         }
-        if (c == 0 && valid) {
+        if (c == 0 && i < n) {
           uint32_t any = 0u;
           for (int t = 0; t < A.kw; ++t) any |= fl[t];
-          if (any) {
+          if (A.priority) {
+            for (int t = 0; t < A.kw; ++t) A.wm[i * A.kw + t] = fl[t];
+            if (any) {
+              const long long pos = (long long)atomicAdd((unsigned long long*)&C->wq_count, 1ull);
+              A.wq[pos] = (int)i;
+            }
+          } else if (any) {
             for (int t = 0; t < A.kw; ++t) A.flipm[i * A.kw + t] = fl[t];
             const long long deg = rp_load(A.rowptr, i + 1) - rp_load(A.rowptr, i);
             const long long nch = deg > kChunk ? (deg + kChunk - 1) / kChunk : 1;
@@ -233,10 +266,49 @@ __global__ void __launch_bounds__(kThreads) ls_kernel(LsArgs<VT, RP, GT> A) {
         }
       }
     }
-    for (int t = 0; t < A.kw; ++t) {
-      int v = cnt[t];
-      for (int o = cp; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if (slot == 0 && v) atomicAdd((unsigned long long*)&s_cnt[32 * t + c], (unsigned long long)v);
+    if (!A.priority) {
+      for (int t = 0; t < A.kw; ++t) {
+        int v = cnt[t];
+        for (int o = cp; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (slot == 0 && v) atomicAdd((unsigned long long*)&s_cnt[32 * t + c], (unsigned long long)v);
+      }
+    } else {
+      if (!grid_barrier(&C->gs)) return;
+      // D2: a wanting node flips the candidates for which no wanting neighbour has a lower rank
+      // (one warp per wanting node; the blocking masks are OR-reduced over the row)
+      const long long nwq = *((volatile long long*)&C->wq_count);
+      int cnt2[4] = {0, 0, 0, 0};
+      for (long long e = gwarp; e < nwq; e += nwarps) {
+        const long long i = (long long)__ldcg(A.wq + e);
+        const int pi = __ldcg(A.prio + i);
+        uint32_t W[4] = {0u, 0u, 0u, 0u}, B[4] = {0u, 0u, 0u, 0u};
+        for (int t = 0; t < A.kw; ++t) W[t] = __ldcg(A.wm + i * A.kw + t);
+        const long long rs = rp_load(A.rowptr, i), re = rp_load(A.rowptr, i + 1);
+        for (long long p = rs + lane; p < re; p += 32) {
+          const int j = __ldg(A.col + p);
+          if (__ldcg(A.prio + j) < pi)
+            for (int t = 0; t < A.kw; ++t) B[t] |= __ldcg(A.wm + (long long)j * A.kw + t);
+        }
+        uint32_t any = 0u;
+        for (int t = 0; t < A.kw; ++t) {
+          B[t] = __reduce_or_sync(0xffffffffu, B[t]);
+          W[t] &= ~B[t];
+          any |= W[t];
+          cnt2[t] += (W[t] >> lane) & 1u;
+        }
+        if (lane == 0 && any) {
+          for (int t = 0; t < A.kw; ++t) {
+            A.flipm[i * A.kw + t] = W[t];
+            if (W[t]) A.sb[i * A.kw + t] = __ldcg(A.sb + i * A.kw + t) ^ W[t];
+          }
+          const long long deg = re - rs;
+          const long long nch = deg > kChunk ? (deg + kChunk - 1) / kChunk : 1;
+          const long long pos = (long long)atomicAdd((unsigned long long*)&C->wl_count, (unsigned long long)nch);
+          for (long long q = 0; q < nch && pos + q < A.wl_cap; ++q) A.wl[pos + q] = (i << 22) | q;
+        }
+      }
+      for (int t = 0; t < A.kw; ++t)
+        if (cnt2[t]) atomicAdd((unsigned long long*)&s_cnt[32 * t + lane], (unsigned long long)cnt2[t]);
     }
     __syncthreads();
     for (int q = threadIdx.x; q < A.k; q += blockDim.x)
@@ -246,16 +318,16 @@ __global__ void __launch_bounds__(kThreads) ls_kernel(LsArgs<VT, RP, GT> A) {
     // U: scatter field changes of the flipped (node, candidate) pairs
     const long long nwl = min(*((volatile long long*)&C->wl_count), A.wl_cap);
     for (long long e = gwarp; e < nwl; e += nwarps) {
-      const long long ent = A.wl[e];
+      const long long ent = __ldcg(A.wl + e);
       const long long i = ent >> 22;
       const long long q = ent & ((1ll << 22) - 1);
       const long long rs = rp_load(A.rowptr, i), re = rp_load(A.rowptr, i + 1);
       const long long cb = rs + q * kChunk;
       const long long ce = (cb + kChunk < re) ? cb + kChunk : re;
       for (int t = 0; t < A.kw; ++t) {
-        const uint32_t F = A.flipm[i * A.kw + t];
+        const uint32_t F = __ldcg(A.flipm + i * A.kw + t);
         if (!F) continue;
-        const uint32_t S = A.sb[i * A.kw + t];
+        const uint32_t S = __ldcg(A.sb + i * A.kw + t);
         const bool mine = (F >> c) & 1u;
         const bool up = (S >> c) & 1u;
         if (!mine) continue;
@@ -279,6 +351,7 @@ __global__ void __launch_bounds__(kThreads) ls_kernel(LsArgs<VT, RP, GT> A) {
             }
             C->total_flips += tot;
             C->wl_count = 0;
+            C->wq_count = 0;
             if (C->phase == 0) {
               C->it += 1;
               const bool any_active = (C->active[0] | C->active[1] | C->active[2] | C->active[3]) != 0u;
@@ -310,7 +383,7 @@ __global__ void __launch_bounds__(kThreads) ls_kernel(LsArgs<VT, RP, GT> A) {
     const long long cq = pr / A.W, wd = pr % A.W;
     const long long i = wd * 32 + lane;
     bool bit = false;
-    if (i < n) bit = (A.sb[i * A.kw + (cq >> 5)] >> (cq & 31)) & 1u;
+    if (i < n) bit = (__ldcg(A.sb + i * A.kw + (cq >> 5)) >> (cq & 31)) & 1u;
     const uint32_t word = __ballot_sync(0xffffffffu, bit);
     if (lane == 0) A.refined[cq * A.W + wd] = word;
   }
@@ -338,6 +411,13 @@ static int launch_ls(sa_handle* h, const sa_ls_params* p, char* ws, int kp, int 
   const size_t o_fm = L.off(sizeof(uint32_t) * (size_t)h->n * kw);
   const size_t o_h = L.off(sizeof(GT) * (size_t)h->n * kp);
   const size_t o_wl = L.off(sizeof(long long) * (size_t)wl_cap);
+  const size_t o_wm = L.off(sizeof(uint32_t) * (size_t)h->n * kw);
+  const size_t o_pr = L.off(sizeof(int) * (size_t)h->n);
+  const size_t o_wq = L.off(sizeof(int) * (size_t)h->n);
+  A.wm = (uint32_t*)(ws + o_wm);
+  A.prio = (int*)(ws + o_pr);
+  A.wq = (int*)(ws + o_wq);
+  A.priority = p->semantics == 0 ? 1 : 0;
   A.ctrl = (LsCtrl*)(ws + o_ctrl);
   A.ebefore = (typename LsArgs<VT, RP, GT>::EAccPtr)(ws + o_eb);
   A.eafter = (typename LsArgs<VT, RP, GT>::EAccPtr)(ws + o_ea);
@@ -358,6 +438,7 @@ static int launch_ls(sa_handle* h, const sa_ls_params* p, char* ws, int kp, int 
   void* args[] = {&A};
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)ls_kernel<VT, RP, GT>, dim3(h->blocks),
                                               dim3(kThreads), args, 0, h->stream);
+  count_launches(1);
   return e == cudaSuccess ? SA_OK : SA_ERR_CUDA;
 }
 
@@ -380,6 +461,9 @@ size_t ls_workspace_bytes(long long n, long long nnz, int k, int integer) {
   L.off(sizeof(uint32_t) * (size_t)n * kw);
   L.off((integer ? sizeof(int) : sizeof(double)) * (size_t)n * kp);
   L.off(sizeof(long long) * (size_t)wl_cap);
+  L.off(sizeof(uint32_t) * (size_t)n * kw);
+  L.off(sizeof(int) * (size_t)n);
+  L.off(sizeof(int) * (size_t)n);
   return L.total;
 }
 

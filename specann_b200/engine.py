@@ -59,6 +59,10 @@ class Engine:
         self.h = h
         self.ls_workspace = None
         self.info: Optional[MatrixInfo] = None
+        # optional per-kernel timing (CUDA events on the engine's stream) for roofline reports
+        self.profile = False
+        self.stats = {"alpha_ms": 0.0, "alpha_bytes": 0.0, "alpha_launches": 0, "spmvs": 0,
+                      "ls_ms": 0.0, "ls_launches": 0}
 
     def close(self):
         if getattr(self, "h", None):
@@ -113,7 +117,18 @@ class Engine:
                         stream_id=int(stream_id), v0=C.c_void_p(v0.data_ptr()) if v0 is not None else None,
                         round=int(bool(round_spins)), residual_check=int(bool(residual_check)))
         rec = AlphaRecord()
+        if self.profile:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(self.stream)
         check("sa_alpha_solve", self.lib.sa_alpha_solve(self.h, C.byref(p), C.byref(rec)))
+        if self.profile:
+            e1.record(self.stream)
+            e1.synchronize()
+            self.stats["alpha_ms"] += e0.elapsed_time(e1)
+            self.stats["alpha_bytes"] += rec.alg_bytes
+            self.stats["alpha_launches"] += 1
+            self.stats["spmvs"] += rec.spmv_count
         return rec
 
     def result_vector(self) -> torch.Tensor:
@@ -171,17 +186,28 @@ class Engine:
         return (base + 255) & ~255, int(nbytes.value)
 
     def local_search(self, k: int, *, first_slot=0, max_iterations=1000, subset_fraction=0.9,
-                     final_sweep_fraction=1.0, final_sweep_iters=25, num_rounds=25, seed=0):
+                     final_sweep_fraction=1.0, final_sweep_iters=25, num_rounds=25, seed=0,
+                     semantics: str = "priority"):
         ptr, nbytes = self._ls_ws(k)
         p = LsParams(k=int(k), first_slot=int(first_slot), max_iterations=int(max_iterations),
                      subset_fraction=float(subset_fraction),
                      final_sweep_fraction=float(final_sweep_fraction), final_sweep_iters=int(final_sweep_iters),
-                     num_rounds=int(num_rounds), seed=int(seed) & (2 ** 64 - 1))
+                     num_rounds=int(num_rounds), seed=int(seed) & (2 ** 64 - 1),
+                     semantics={"priority": 0, "snapshot": 1}[semantics])
         eb = (C.c_double * k)()
         ea = (C.c_double * k)()
         res = LsResult()
+        if self.profile:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(self.stream)
         check("sa_local_search", self.lib.sa_local_search(self.h, C.byref(p), C.c_void_p(ptr), nbytes, eb, ea,
                                                           C.byref(res)))
+        if self.profile:
+            e1.record(self.stream)
+            e1.synchronize()
+            self.stats["ls_ms"] += e0.elapsed_time(e1)
+            self.stats["ls_launches"] += 1
         return np.array(eb[:]), np.array(ea[:]), res
 
     def energies(self, k: int) -> np.ndarray:

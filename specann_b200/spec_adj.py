@@ -49,6 +49,7 @@ class _FixedAlpha:
         self.dtype = np.float32 if self.precision == 32 else np.float64
         self.solver_name = run_name if run_name else self._default_name
         self.verbose = bool(kwargs.pop("verbose", False))
+        self.ls_semantics = str(kwargs.pop("ls_semantics", "priority"))
         self.engine = None
 
     def _solve_eigen(self, eng, n):
@@ -87,7 +88,8 @@ class _FixedAlpha:
         local_iterations = 0
         use_refined = False
         if self.use_local_search:
-            eb, ea, res = eng.local_search(1, max_iterations=self.max_local_iterations, seed=self._seed)
+            eb, ea, res = eng.local_search(1, max_iterations=self.max_local_iterations, seed=self._seed,
+                                           semantics=self.ls_semantics)
             local_iterations = int(res.iterations)
             energy = float(eb[0])
             if ea[0] < eb[0]:

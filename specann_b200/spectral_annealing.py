@@ -153,6 +153,13 @@ class SpectralAnnealing:
         self.solver_name = run_name if run_name else "spectral_annealing_pred"
         self.residual_check = bool(kwargs.pop("residual_check", True))
         self.verbose = bool(kwargs.pop("verbose", False))
+        # write_results=False skips the result CSVs (the reference writes them after its timer)
+        self.write_results = bool(kwargs.pop("write_results", True))
+        self.profile = bool(kwargs.pop("profile", False))
+        # local-search pass semantics: "priority" (independent flips, monotone) or "snapshot"
+        self.ls_semantics = str(kwargs.pop("ls_semantics", "priority"))
+        if self.ls_semantics not in ("priority", "snapshot"):
+            raise ValueError(f"ls_semantics must be 'priority' or 'snapshot', got {self.ls_semantics!r}")
         self._extra_kwargs = kwargs
         self.engine = None
         if self.verbose:
@@ -214,23 +221,48 @@ class SpectralAnnealing:
     def solve(self, J):
         """Run SpecAnn on J (SciPy CSR or dense, symmetric, zero diagonal); write the CSVs.
         Returns (best energy, best spins as a NumPy array of +-1 in the solver dtype, seconds)."""
-        from .engine import Engine
         start_time = time.time()
+        self._check_runnable()
+        Jc = as_csr(J)
+        n = Jc.shape[0]
+        eng = self._make_engine(n, Jc.nnz)
+        data = Jc.data.astype(np.float32) if (self.precision == 32) else Jc.data
+        info = eng.upload_csr(Jc.indptr, Jc.indices, data)
+        return self._sweep(eng, info, Jc, start_time)
+
+    def solve_device(self, rowptr, col, val):
+        """The same solve on a CSR already in device memory (torch CUDA tensors: row pointers int32
+        or int64, columns int32, couplings float32 at precision 32 / float64 at 64). The reported
+        energy is the device energy of the best spins (exact for integer couplings)."""
+        start_time = time.time()
+        self._check_runnable()
+        n = int(rowptr.numel()) - 1
+        eng = self._make_engine(n, int(col.numel()))
+        info = eng.bind(rowptr, col, val)
+        return self._sweep(eng, info, None, start_time)
+
+    def _check_runnable(self):
         if self.alpha is not None:
             raise ValueError("Alpha is not set")
         if self.ls_policy != "default" and self.use_local_search:
             raise NotImplementedError(f"ls_policy {self.ls_policy!r} (guarded local search) is not part of the "
                                       f"B200 engine; use ls_policy='default'")
-        Jc = as_csr(J)
-        n = Jc.shape[0]
+
+    def _make_engine(self, n, nnz):
+        from .engine import Engine
         self._seed = _seed_value(self.random_seed)
         eng_prec = 32 if self.fp32_spmv else 64
-        data = Jc.data.astype(np.float32) if (self.precision == 32) else Jc.data
-        capacity = min(128, self.num_alphas)
-        ncv = default_ncv(n, self.eigsh_ncv)
-        eng = Engine(n, Jc.nnz, precision=eng_prec, ncv_max=max(ncv, 2), max_candidates=capacity)
+        self._capacity = min(128, self.num_alphas)
+        self._ncv = default_ncv(n, self.eigsh_ncv)
+        eng = Engine(n, nnz, precision=eng_prec, ncv_max=max(self._ncv, 2), max_candidates=self._capacity)
+        eng.profile = self.profile
         self.engine = eng
-        info = eng.upload_csr(Jc.indptr, Jc.indices, data)
+        return eng
+
+    def _sweep(self, eng, info, Jc, start_time):
+        n = eng.n
+        ncv = self._ncv
+        capacity = self._capacity
         self._normalization_factor = info.c
         alpha_list = self._get_alpha_values(self.mode)
         cands = _Candidates(eng, capacity)
@@ -312,7 +344,7 @@ class SpectralAnnealing:
             kind, c = best_src
             best_spins = eng.candidate_spins(c, refined=(kind == 'refined')).cpu().numpy().astype(self.dtype)
         total_time = time.time() - start_time
-        if best_spins is not None:
+        if best_spins is not None and Jc is not None:
             s64 = best_spins.astype(np.float64)
             best_energy = float(-0.5 * s64 @ (Jc @ s64))
         self._sweep_time = sweep_end - start_time
@@ -320,27 +352,32 @@ class SpectralAnnealing:
         import torch
         self._gpu_pool_bytes = int(torch.cuda.memory_reserved())
         if best_alpha is None:
-            self._store_timing_results(alpha_results)
+            if self.write_results:
+                self._store_timing_results(alpha_results)
             message = f"no alpha produced a solution ({self._alphas_skipped} of {len(alpha_list)} skipped)"
             if self._alpha_errors:
                 last = self._last_alpha_error
                 raise RuntimeError(f"{message}; {self._alpha_errors} of them raised a non-numerical error, "
                                    f"the last {type(last).__name__}: {last}") from last
             raise NumericalFailure(message)
-        self._store_general_results(best_energy, best_alpha, None, total_time, best_iters)
-        self._store_timing_results(alpha_results)
+        self.alpha_results = alpha_results
+        if self.write_results:
+            self._store_general_results(best_energy, best_alpha, None, total_time, best_iters)
+            self._store_timing_results(alpha_results)
         return best_energy, best_spins, total_time
 
     def _refine(self, eng, k):
         """Local search of the distinct candidates: (energies before, energies after, passes)."""
         if self.ls_batch:
-            eb, ea, res = eng.local_search(k, max_iterations=self.max_local_iterations, seed=self._seed)
+            eb, ea, res = eng.local_search(k, max_iterations=self.max_local_iterations, seed=self._seed,
+                                           semantics=self.ls_semantics)
             return eb, ea, int(res.iterations)
         eb = np.empty(k)
         ea = np.empty(k)
         used = 0
         for c in range(k):
-            b, a, res = eng.local_search(1, first_slot=c, max_iterations=self.max_local_iterations, seed=self._seed)
+            b, a, res = eng.local_search(1, first_slot=c, max_iterations=self.max_local_iterations, seed=self._seed,
+                                         semantics=self.ls_semantics)
             eb[c], ea[c] = b[0], a[0]
             used = max(used, int(res.iterations))
         return eb, ea, used

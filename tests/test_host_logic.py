@@ -128,3 +128,17 @@ def test_oracle_reference_kernel_emulation_counts():
     assert counts.sum() == int((S2 != S).sum())
     # in-place sequential single flips never raise the energy
     assert np.all(O.integer_energies(J, S2) <= O.integer_energies(J, S))
+
+
+def test_priority_local_search_is_monotone_and_stable():
+    """Priority passes: flips form an independent set, so energy never rises and the result is a
+    1-flip local minimum once the final sweep ends without flips."""
+    J = graphs.barabasi_albert(2000, 8, seed=3, couplings="int100")
+    S = np.where(np.random.default_rng(4).random((4, 2000)) < 0.5, 1, -1).astype(np.int8)
+    res = O.local_search(J, S, seed=5)
+    assert np.all(res.energies_after <= res.energies_before)
+    Ji = sp.csr_matrix((np.rint(J.data).astype(np.int64), J.indices, J.indptr), shape=J.shape)
+    H = Ji @ res.spins.T.astype(np.int64)
+    assert np.all(res.spins.T.astype(np.int64) * H >= 0)      # no improving single flip left
+    snap = O.local_search(J, S, seed=5, semantics="snapshot", max_iterations=50, num_rounds=2)
+    assert snap.spins.shape == S.shape

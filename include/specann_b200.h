@@ -175,6 +175,25 @@ int sa_local_search(sa_handle* h, const sa_ls_params* p, void* ls_workspace, siz
  * fp32_energies, models/spectral_annealing.py:693-707, :962-976. */
 int sa_energies(sa_handle* h, int32_t k, void* ls_workspace, size_t ls_bytes, double* energies);
 
+/* ---- allocation-free operator ------------------------------------------------------------- */
+
+/* Largest n accepted by sa_spmv_scaled_noalloc. */
+#define SA_NOALLOC_MAX_N (1 << 20)
+
+/* y = rho x - N_alpha x (the operator of sa_spmv_scaled) for callers that cannot allocate device
+ * memory and have no workspace to hand over, such as a host framework whose pool allocator owns the
+ * whole device, or a latency-sensitive caller that must not pay for cudaMalloc's implicit device
+ * synchronisation. No counterpart in the reference. It needs no handle: the CSR (int32 row pointers,
+ * int32 columns, float couplings; symmetric, zero diagonal), x and y are the caller's device
+ * buffers, and the degrees and scaling are computed on every call. Its scratch is a fixed device
+ * array inside the library (8 MiB per GPU, held until the process exits), so it allocates nothing.
+ * n > SA_NOALLOC_MAX_N is rejected with SA_ERR_INVALID_ARG. The first call on each device looks up
+ * the array's device address; make that first call before any stream capture. All calls share the
+ * array: calls that overlap on the GPU race, so serialise them. */
+int sa_spmv_scaled_noalloc(int64_t n, int64_t nnz, const int32_t* rowptr, const int32_t* col,
+                           const float* val, double alpha, double rho, const float* x, float* y,
+                           void* stream);
+
 /* Version string of the library. */
 const char* sa_version(void);
 

@@ -63,6 +63,8 @@ class LsResult(C.Structure):
 # name -> (restype, argtypes): every symbol include/specann_b200.h declares
 SIGNATURES = {
     "sa_version": (C.c_char_p, []),
+    "sa_spmv_scaled_noalloc": (C.c_int, [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                         C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sa_kernel_launches": (C.c_uint64, []),
     "sa_workspace_size": (C.c_int, [C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                     C.POINTER(C.c_size_t)]),

@@ -45,6 +45,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-alphas", type=int, default=2)
     ap.add_argument("--spmv-reps", type=int, default=20)
+    ap.add_argument("--scale-run", action="store_true",
+                    help="one timed FP32 solve and one timed plain-FP64 solve of the graph, with the energy gap")
+    ap.add_argument("--spmv-only", action="store_true",
+                    help="time only the standalone fused SpMV on the resident matrix (profiling runs)")
     return ap.parse_args()
 
 
@@ -203,6 +207,68 @@ def main():
         if world > 1:
             dist.barrier()
 
+    if args.scale_run:
+        out = {"scale_run": True, "n": n, "nnz": nnz, "workload": f"BA(n=2^{args.log2n}, m={args.m}) J=-A, "
+                                                                  f"{args.num_alphas} alphas sqrt schedule"}
+        # load the kernels once on a small graph (not timed)
+        from specann_b200 import graphs as _g
+        Jw = _g.barabasi_albert(4096, 8, seed=1)
+        SpectralAnnealing("w.txt", "w", random_seed=1, num_alphas=4, write_results=False).solve(Jw)
+        d_val64 = None
+        for prec in (32, 64):
+            if prec == 64:
+                del d_val
+                torch.cuda.empty_cache()
+                d_val64 = torch.from_numpy(val.astype(np.float64)).to(dev)
+            vv = d_val if prec == 32 else d_val64
+            s = SpectralAnnealing("scale.txt", "scale", random_seed=42, num_alphas=args.num_alphas, precision=prec,
+                                  write_results=False, profile=True)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            e, spins, _ = s.solve_device(d_rowptr, d_col, vv)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            st = s.engine.stats
+            iters = [r["eigsh_iterations"] for r in s.alpha_results]
+            out[f"fp{prec}"] = {"seconds": dt, "best_energy": e, "spmvs": st["spmvs"],
+                                "alpha_kernel_s": st["alpha_ms"] / 1e3, "ls_kernel_s": st["ls_ms"] / 1e3,
+                                "alpha_GBps": st["alpha_bytes"] / (st["alpha_ms"] / 1e3) / 1e9,
+                                "phase_s": [round(x / 1e3, 3) for x in st.get("phase_ms", [0] * 6)],
+                                "iters_mean": float(np.mean(iters)), "iters_max": int(np.max(iters)),
+                                "max_residual": float(np.nanmax([r["eigsh_residual"] for r in s.alpha_results])),
+                                "candidates": int(s._num_candidates or 0),
+                                "peak_mem_gb": torch.cuda.max_memory_allocated() / 1e9}
+            del s
+            torch.cuda.empty_cache()
+            print(json.dumps(out), flush=True)
+        e32, e64 = out["fp32"]["best_energy"], out["fp64"]["best_energy"]
+        out["energy_gap_rel"] = abs(e32 - e64) / abs(e64)
+        print(json.dumps(out))
+        return
+
+    if args.spmv_only:
+        from specann_b200.engine import Engine
+        eng = Engine(n, nnz, precision=args.precision, ncv_max=33, max_candidates=1)
+        eng.bind(d_rowptr, d_col, d_val)
+        x = torch.randn(n, device=dev, dtype=torch.float32 if args.precision == 32 else torch.float64)
+        y = torch.empty_like(x)
+        for _ in range(args.warmup):
+            eng.spmv(0.5, 1.001, x, y)
+        torch.cuda.synchronize()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(args.spmv_reps):
+            eng.spmv(0.5, 1.001, x, y)
+        s1.record()
+        torch.cuda.synchronize()
+        ms_ = s0.elapsed_time(s1) / args.spmv_reps
+        sb_ = spmv_bytes(n, nnz, rp_np.itemsize, t)
+        hbm_, kind_ = peaks()
+        print(json.dumps({"spmv_only": True, "n": n, "nnz": nnz, "ms": ms_, "bytes": sb_,
+                          "GBps": sb_ / ms_ / 1e6, "frac": sb_ / ms_ / 1e6 / hbm_, "peak_source": kind_}))
+        return
+
     # warm-up (untimed), then K timed steps with the CSR resident in HBM
     for _ in range(args.warmup):
         solver().solve_device(d_rowptr, d_col, d_val)
@@ -241,7 +307,8 @@ def main():
         with open(os.environ["SPECANN_BENCH_DUMP"], "w") as f:
             for r in s.alpha_results:
                 f.write(json.dumps({k: r[k] for k in ("alpha", "eigsh_iterations", "eigsh_restarts", "eigsh_residual",
-                                                      "lambda1", "pred_accepted", "pred_residual", "candidate")}) + "\n")
+                                                      "lambda1", "pred_accepted", "pred_residual", "candidate",
+                                                      "eigsh_spmvs", "alg_bytes")}) + "\n")
     lanczos = {"mean": float(iters.mean()), "median": float(np.median(iters)), "max": float(iters.max()),
                "alpha0": float(iters[0]), "restarts": int(sum(r["eigsh_restarts"] for r in s.alpha_results)),
                "pred_accepted": int(sum(1 for r in s.alpha_results if r["pred_accepted"])),
@@ -303,6 +370,8 @@ def main():
                      "peak_source": peak_kind,
                      "alpha_kernel_ms_per_solve": st["alpha_ms"], "alpha_launches_per_solve": st["alpha_launches"],
                      "spmvs_per_solve": st["spmvs"], "ls_kernel_ms_per_solve": st["ls_ms"],
+                     "alpha_phase_ms": dict(zip(("setup", "spmv", "dots", "update_ritz", "restart", "final"),
+                                               [round(x, 3) for x in st.get("phase_ms", [0.0] * 6)])),
                      "lanczos_iterations": lanczos},
         "spmv": {"achieved": spmv_gbs, "peak": hbm, "unit": "GB/s", "frac": spmv_gbs / hbm,
                  "ms": spmv_ms, "bytes": sb},

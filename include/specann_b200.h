@@ -79,6 +79,7 @@ typedef struct {
   int32_t spmv_count;    /* fused SpMVs the launch ran (Lanczos steps, predictor test, residual) */
   int32_t reserved;
   double alg_bytes;      /* algorithmic DRAM bytes of the launch: SpMVs + basis/vector passes */
+  double phase_ms[6];    /* device time by phase: set-up, SpMV, dots, update+Ritz, restart, final */
 } sa_alpha_record;
 
 typedef struct {

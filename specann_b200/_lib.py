@@ -44,7 +44,7 @@ class AlphaRecord(C.Structure):
                 ("residual", C.c_double), ("res_estimate", C.c_double), ("pred_residual", C.c_double),
                 ("degree_scale", C.c_double), ("align_dot", C.c_double), ("signature", C.c_uint64),
                 ("nonfinite", C.c_int32), ("basis_used", C.c_int32), ("spmv_count", C.c_int32),
-                ("reserved", C.c_int32), ("alg_bytes", C.c_double)]
+                ("reserved", C.c_int32), ("alg_bytes", C.c_double), ("phase_ms", C.c_double * 6)]
 
 
 class LsParams(C.Structure):

@@ -20,7 +20,7 @@ CSRC = PKG / "csrc"
 CUDA_LIB = "libspecann_b200.so"
 GRAPH_LIB = "libspecann_graphs.so"
 CU_SOURCES = ["capi.cu", "alpha.cu", "ls.cu", "noalloc.cu"]
-HEADERS = ["common.cuh", "handle.cuh", "spmv.cuh"]
+HEADERS = ["common.cuh", "handle.cuh", "spmv.cuh", "policy.cuh", "alpha_body.cuh", "ls_body.cuh"]
 
 
 def nvcc_path() -> str:

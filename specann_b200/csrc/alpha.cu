@@ -1,762 +1,11 @@
-// One alpha of the SpecAnn sweep as one persistent cooperative kernel: start vector / predictor,
-// warm-started thick-restart Lanczos for the smallest eigenpair of S_rho = rho I - N_alpha with
-// FP64 inner products and an FP64 tridiagonal Ritz solve, the Ritz-matrix guard, sign alignment,
-// the true residual, and rounding to packed spins with an order-independent signature.
-//
-// CTAs rewrite V, w, u and y between phases and the per-SM L1 is not coherent with writes from
-// other SMs, so every read of those arrays inside this kernel uses ld.global.cg (L2).
-//
-// Vectors (basis V, w, u, y) are in T (float or double); every inner product and norm is
-// accumulated in double; the projected tridiagonal T_j lives in double in the control block.
-// Between phases the CTAs meet at grid_barrier, whose epilogue (run by the last CTA to arrive)
-// reduces the per-CTA partial sums in CTA order and takes the Lanczos decisions, so every CTA
-// follows the same control path and results do not depend on timing.
-#include <cmath>
-#include <cstdio>
-
-#include "common.cuh"
-#include "handle.cuh"
-#include "spmv.cuh"
+// Host launch of the single-problem alpha solve (cooperative grid; device code in alpha_body.cuh).
+#include "alpha_body.cuh"
 
 namespace sa {
 
-void count_launches(int k);
-
-enum Action : int { ACT_NEXT = 0, ACT_REPASS = 1, ACT_RESTART = 2, ACT_REJECT = 3, ACT_DONE = 4, ACT_ERROR = 5,
-                    ACT_P0_AGAIN = 6 };
-
-constexpr double kLog2Clamp = -39.86313713864835;   // log2(1e-12)
-constexpr double kTinyNorm = 1e-12;
-
 template <typename T, typename RP>
-struct AlphaArgs {
-  SpmvArgs<T, RP> S;
-  long long n, ldv;
-  T* sigma;
-  const double* ld;
-  T* V;
-  T* w;
-  T* u;
-  const T* ylast;
-  const T* yprev;
-  T* yout;
-  const T* v0;
-  double* part;          // per-CTA partial sums, blocks x pw
-  int pw;
-  AlphaCtrl* ctrl;
-  uint32_t* bits;        // scratch candidate (W words)
-  long long W;
-  sa_alpha_params p;
-  int has_last, has_prev;
-  double half_log2_c;
-  double sqrt_c;
-  int group;
-  double spmv_bytes;     // algorithmic bytes of one fused SpMV
-  double* dense;         // implicit-restart scratch (dense T, then dense Q)
-};
-
-// ---- small dense helpers for the projected tridiagonal (double, one CTA) --------------------
-
-// Number of eigenvalues of the tridiagonal (a, b; size m) below x: sign changes of the leading
-// principal minors det(T_k - x I), computed with the three-term recurrence and rescaling.
-__device__ int sturm_count(const double* a, const double* b, int m, double x) {
-  double pp = 1.0, pc = a[0] - x;
-  bool neg = pc < 0.0;
-  int cnt = neg ? 1 : 0;
-  for (int i = 1; i < m; ++i) {
-    const double pn = (a[i] - x) * pc - b[i - 1] * b[i - 1] * pp;
-    pp = pc;
-    pc = pn;
-    const double mag = fabs(pc);
-    if (mag > 1e200) { pc *= 1e-200; pp *= 1e-200; }
-    else if (mag < 1e-200 && fabs(pp) < 1e-200) { pc *= 1e200; pp *= 1e200; }
-    const bool nneg = (pc != 0.0) ? (pc < 0.0) : !neg;
-    cnt += (nneg != neg);
-    neg = nneg;
-  }
-  return cnt;
-}
-
-// s_last^2 of the unit eigenvector for eigenvalue x: -det(T_{m-1} - x) / det'(T_m - x).
-__device__ double last_component_sq(const double* a, const double* b, int m, double x) {
-  double pp = 1.0, pc = a[0] - x, dp = 0.0, dc = -1.0;
-  for (int i = 1; i < m; ++i) {
-    const double bb = b[i - 1] * b[i - 1];
-    const double pn = (a[i] - x) * pc - bb * pp;
-    const double dn = -pc + (a[i] - x) * dc - bb * dp;
-    pp = pc; pc = pn; dp = dc; dc = dn;
-    const double mag = fmax(fmax(fabs(pc), fabs(dc)), fmax(fabs(pp), fabs(dp)));
-    if (mag > 1e200) { pc *= 1e-200; pp *= 1e-200; dc *= 1e-200; dp *= 1e-200; }
-    else if (mag < 1e-200 && mag > 0.0) { pc *= 1e200; pp *= 1e200; dc *= 1e200; dp *= 1e200; }
-  }
-  // pp = det(T_{m-1} - x) (1 for m = 1), dc = det'(T_m - x)
-  if (dc == 0.0) return 1.0;
-  double s2 = -pp / dc;
-  if (!(s2 >= 0.0)) s2 = 0.0;
-  if (s2 > 1.0) s2 = 1.0;
-  return s2;
-}
-
-// Smallest eigenvalue by multisection over the whole CTA (blockDim.x points per round).
-__device__ double smallest_eig_block(const double* a, const double* b, int m) {
-  __shared__ double s_lo, s_hi;
-  __shared__ int s_first;
-  if (threadIdx.x == 0) {
-    double lo = 1e300, hi = -1e300;
-    for (int i = 0; i < m; ++i) {
-      const double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i + 1 < m ? fabs(b[i]) : 0.0);
-      lo = fmin(lo, a[i] - r);
-      hi = fmax(hi, a[i] + r);
-    }
-    const double pad = 1e-12 * fmax(1.0, fmax(fabs(lo), fabs(hi)));
-    s_lo = lo - pad;
-    s_hi = hi + pad;
-  }
-  __syncthreads();
-  const int P = blockDim.x;
-  for (int round = 0; round < 7; ++round) {
-    const double lo = s_lo, hi = s_hi;
-    if (threadIdx.x == 0) s_first = P;
-    __syncthreads();
-    const double x = lo + (hi - lo) * (double)(threadIdx.x + 1) / (double)(P + 1);
-    if (sturm_count(a, b, m, x) >= 1) atomicMin(&s_first, (int)threadIdx.x);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const int f = s_first;
-      const double nlo = (f == 0) ? lo : lo + (hi - lo) * (double)f / (double)(P + 1);
-      const double nhi = (f >= P) ? hi : lo + (hi - lo) * (double)(f + 1) / (double)(P + 1);
-      s_lo = nlo;
-      s_hi = nhi;
-    }
-    __syncthreads();
-    if (s_hi - s_lo <= 1e-15 * fmax(1.0, fabs(s_hi))) break;
-  }
-  const double r = 0.5 * (s_lo + s_hi);
-  __syncthreads();
-  return r;
-}
-
-// Unit eigenvector of the tridiagonal for eigenvalue theta by inverse iteration (one thread):
-// LU with partial pivoting of (T - theta I), two solves from a constant start.
-__device__ void tridiag_eigvec(const double* a, const double* b, int m, double theta, double* s) {
-  if (m == 1) { s[0] = 1.0; return; }
-  double dl[kNcvMax], d[kNcvMax], du[kNcvMax], du2[kNcvMax];
-  int ipiv[kNcvMax];
-  double anorm = 0.0;
-  for (int i = 0; i < m; ++i) {
-    d[i] = a[i] - theta;
-    if (i + 1 < m) { dl[i] = b[i]; du[i] = b[i]; }
-    anorm = fmax(anorm, fabs(a[i]) + (i > 0 ? fabs(b[i - 1]) : 0.0) + (i + 1 < m ? fabs(b[i]) : 0.0));
-  }
-  const double tiny = fmax(anorm, 1e-300) * 1e-15;
-  for (int i = 0; i < m; ++i) du2[i] = 0.0;
-  for (int i = 0; i < m - 1; ++i) {
-    if (fabs(d[i]) >= fabs(dl[i])) {
-      ipiv[i] = i;
-      if (d[i] == 0.0) d[i] = tiny;
-      const double f = dl[i] / d[i];
-      dl[i] = f;
-      d[i + 1] -= f * du[i];
-    } else {
-      ipiv[i] = i + 1;
-      const double f = d[i] / dl[i];
-      d[i] = dl[i];
-      dl[i] = f;
-      const double t = du[i];
-      du[i] = d[i + 1];
-      d[i + 1] = t - f * d[i + 1];
-      if (i < m - 2) {
-        du2[i] = du[i + 1];
-        du[i + 1] = -f * du[i + 1];
-      }
-    }
-  }
-  ipiv[m - 1] = m - 1;
-  if (d[m - 1] == 0.0) d[m - 1] = tiny;
-  for (int i = 0; i < m; ++i) s[i] = 1.0;
-  for (int iter = 0; iter < 3; ++iter) {
-    // forward: L
-    for (int i = 0; i < m - 1; ++i) {
-      if (ipiv[i] == i) {
-        s[i + 1] -= dl[i] * s[i];
-      } else {
-        const double t = s[i];
-        s[i] = s[i + 1];
-        s[i + 1] = t - dl[i] * s[i];
-      }
-    }
-    // backward: U
-    s[m - 1] /= d[m - 1];
-    if (m > 1) s[m - 2] = (s[m - 2] - du[m - 2] * s[m - 1]) / d[m - 2];
-    for (int i = m - 3; i >= 0; --i) s[i] = (s[i] - du[i] * s[i + 1] - du2[i] * s[i + 2]) / d[i];
-    double nrm = 0.0;
-    for (int i = 0; i < m; ++i) nrm += s[i] * s[i];
-    nrm = sqrt(nrm);
-    if (!(nrm > 0.0) || !isfinite(nrm)) { for (int i = 0; i < m; ++i) s[i] = (i == 0) ? 1.0 : 0.0; return; }
-    for (int i = 0; i < m; ++i) s[i] /= nrm;
-  }
-}
-
-// The (q+1)-th smallest eigenvalue of the tridiagonal by bisection on the Sturm count.
-__device__ double kth_eig(const double* a, const double* b, int m, int q) {
-  double lo = 1e300, hi = -1e300;
-  for (int i = 0; i < m; ++i) {
-    const double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i + 1 < m ? fabs(b[i]) : 0.0);
-    lo = fmin(lo, a[i] - r);
-    hi = fmax(hi, a[i] + r);
-  }
-  lo -= 1e-12 * fmax(1.0, fabs(lo));
-  hi += 1e-12 * fmax(1.0, fabs(hi));
-  for (int it = 0; it < 80 && hi - lo > 1e-15 * fmax(1.0, fabs(hi)); ++it) {
-    const double mid = 0.5 * (lo + hi);
-    if (sturm_count(a, b, m, mid) >= q + 1) hi = mid;
-    else lo = mid;
-  }
-  return 0.5 * (lo + hi);
-}
-
-// Implicit restart with exact shifts (the CTA): the m - kk largest Ritz values of the tridiagonal
-// (a, b; size m) are the shifts of implicit QR steps, done as Givens bulge chasing on a dense copy
-// Td with the rotations accumulated in Qd (both m x m, row-major). Afterwards Qd^T T Qd has a
-// leading kk x kk tridiagonal, written back to a and b, and the residual of the kept basis is
-// V Q[:, kk] T+[kk][kk-1] + w Q[m-1][kk-1] (w: the pending unnormalised Lanczos vector).
-__device__ void implicit_restart(AlphaCtrl* C, double* Td, double* Qd, int m, int kk) {
-  __shared__ double s_ritz[kNcvMax];
-  __shared__ double s_c, s_s;
-  const int t = threadIdx.x;
-  if (t < m) s_ritz[t] = kth_eig(C->a, C->b, m, t);
-  for (int idx = t; idx < m * m; idx += blockDim.x) {
-    const int r = idx / m, c = idx % m;
-    double v = 0.0;
-    if (r == c) v = C->a[r];
-    else if (r == c + 1) v = C->b[c];
-    else if (c == r + 1) v = C->b[r];
-    Td[idx] = v;
-    Qd[idx] = (r == c) ? 1.0 : 0.0;
-  }
-  __syncthreads();
-  for (int sft = m - 1; sft >= kk; --sft) {
-    const double mu = s_ritz[sft];
-    for (int r = 0; r < m - 1; ++r) {
-      if (t == 0) {
-        const double x = (r == 0) ? Td[0] - mu : Td[r * m + (r - 1)];
-        const double z = (r == 0) ? Td[m] : Td[(r + 1) * m + (r - 1)];
-        const double rr = hypot(x, z);
-        s_c = (rr == 0.0) ? 1.0 : x / rr;
-        s_s = (rr == 0.0) ? 0.0 : z / rr;
-      }
-      __syncthreads();
-      const double c = s_c, s = s_s;
-      if (t < m) {
-        const double p = Td[r * m + t], q = Td[(r + 1) * m + t];
-        Td[r * m + t] = c * p + s * q;
-        Td[(r + 1) * m + t] = -s * p + c * q;
-      }
-      __syncthreads();
-      if (t < m) {
-        double p = Td[t * m + r], q = Td[t * m + r + 1];
-        Td[t * m + r] = c * p + s * q;
-        Td[t * m + r + 1] = -s * p + c * q;
-        p = Qd[t * m + r];
-        q = Qd[t * m + r + 1];
-        Qd[t * m + r] = c * p + s * q;
-        Qd[t * m + r + 1] = -s * p + c * q;
-      }
-      __syncthreads();
-    }
-  }
-  if (t < kk) {
-    C->a[t] = Td[t * m + t];
-    if (t + 1 < kk) C->b[t] = Td[(t + 1) * m + t];
-  }
-  if (t == 0) {
-    C->irl_beta = Td[kk * m + (kk - 1)];
-    C->irl_sigma = Qd[(m - 1) * m + (kk - 1)];
-    C->irl_k = kk;
-  }
-  __syncthreads();
-}
-
-// ---- reductions of per-CTA partials --------------------------------------------------------
-
-// Sum part[blk * pw + col] over blocks for cols [0, ncols) into out[col] (fixed order).
-__device__ void reduce_partials(const double* part, int pw, int nblocks, int ncols, double* out) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int c = wid; c < ncols; c += nw) {
-    double acc = 0.0;
-    for (int bk = lane; bk < nblocks; bk += 32) acc += *((volatile const double*)(part + (long long)bk * pw + c));
-    acc = warp_sum(acc);
-    if (lane == 0) out[c] = acc;
-  }
-  __syncthreads();
-}
-
-// Block-reduce NV per-thread values and store them as this CTA's partials [col0, col0 + NV).
-template <int NV>
-__device__ void block_store_partials(const double (&v)[NV], double* part, int pw, int col0, double* sm) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  double r[NV];
-#pragma unroll
-  for (int q = 0; q < NV; ++q) r[q] = warp_sum(v[q]);
-  __syncthreads();
-  if (lane == 0) {
-#pragma unroll
-    for (int q = 0; q < NV; ++q) sm[wid * NV + q] = r[q];
-  }
-  __syncthreads();
-  if (threadIdx.x < NV) {
-    double acc = 0.0;
-    for (int wv = 0; wv < nw; ++wv) acc += sm[wv * NV + threadIdx.x];
-    part[(long long)blockIdx.x * pw + col0 + threadIdx.x] = acc;
-  }
-  __syncthreads();
-}
-
-template <typename T>
-__device__ __forceinline__ T vload(const T* p) { return *((volatile const T*)p); }
-
-__device__ __forceinline__ unsigned long long word_mix(long long widx, unsigned int word) {
-  return splitmix64(((unsigned long long)widx << 32) ^ (unsigned long long)word ^ 0xA5A5000000000000ull);
-}
-
-// ---- the alpha-solve kernel ----------------------------------------------------------------
-
-template <typename T, typename RP>
-__global__ void __launch_bounds__(kThreads, 2) alpha_kernel(AlphaArgs<T, RP> A) {
-  __shared__ double sm[kWarps * (kDotBatch + 1)];
-  __shared__ double sh[kNcvMax];
-  __shared__ double s_theta, s_s2;
-  __shared__ SpmvSmem<T> ssp;
-  __shared__ double sq[kNcvMax * (kDotBatch + 1)];
-  AlphaCtrl* C = A.ctrl;
-  const long long n = A.n;
-  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long nthreads = (long long)gridDim.x * blockDim.x;
-  const long long gwarp = gtid >> 5, nwarps = nthreads >> 5;
-  const sa_alpha_params& P = A.p;
-  const double rho = P.rho;
-  const double bound = 10.0 * (P.rho + P.gershgorin);
-  const int ncv = P.ncv;
-
-  // ---------------- P0: sigma, degree scale, start vector --------------------------------------
-  int mode = P.start_mode;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    C->mode = mode;
-    C->test_pred = (mode == SA_START_DIAGONAL || mode == SA_START_SECANT) ? 1 : 0;
-    C->pred_accepted = -1;
-    C->pred_residual = nan("");
-    C->iters = 0;
-    C->restarts = 0;
-    C->status = SA_OK;
-    C->nonfinite = 0;
-    C->sig = 0ull;
-    C->secant_sign = 1;
-    C->bytes = 0.0;
-    C->spmvs = 0;
-  }
-  {
-    double ds = 0.0;
-    for (long long i = gtid; i < n; i += nthreads) {
-      const double ldi = (double)A.ld[i];
-      const double logD = (P.alpha == 0.0) ? 0.0 : P.alpha * ldi;
-      const double logDc = fmax(logD, kLog2Clamp);
-      A.sigma[i] = (T)exp2(-0.5 * logDc - A.half_log2_c);
-      ds += exp2(logD);
-    }
-    double v[1] = {ds};
-    block_store_partials<1>(v, A.part, A.pw, 0, sm);
-  }
-  if (!grid_barrier(&C->gs, [&] {
-        reduce_partials(A.part, A.pw, gridDim.x, 1, sh);
-        if (threadIdx.x == 0) {
-          C->degree_scale = sh[0];
-          C->bytes += (double)n * (8.0 + sizeof(T));
-        }
-      })) return;
-
-  if (mode == SA_START_SECANT && A.has_prev) {
-    double v[1] = {0.0};
-    for (long long i = gtid; i < n; i += nthreads) v[0] += (double)A.ylast[i] * (double)A.yprev[i];
-    block_store_partials<1>(v, A.part, A.pw, 0, sm);
-    if (!grid_barrier(&C->gs, [&] {
-          reduce_partials(A.part, A.pw, gridDim.x, 1, sh);
-          if (threadIdx.x == 0) {
-            C->secant_sign = (sh[0] < 0.0) ? -1 : 1;
-            C->bytes += 2.0 * (double)n * sizeof(T);
-          }
-        })) return;
-  }
-
-  while (true) {   // P0 loop (repeats for a predictor fallback or rejection)
-    mode = vload(&C->mode);
-    const int sgn = vload(&C->secant_sign);
-    const unsigned long long key = splitmix64(P.seed ^ 0x57A27000ull) ^ splitmix64((unsigned long long)P.stream_id + 0x1234567ull);
-    double v[3] = {0.0, 0.0, 0.0};   // ||v0||^2, ||s||^2 (secant), ||y||^2 (secant)
-    for (long long i = gtid; i < n; i += nthreads) {
-      double x;
-      if (mode == SA_START_RANDOM) {
-        x = (double)(T)normal_from_counter(key, i);
-      } else if (mode == SA_START_PREV) {
-        x = (double)A.ylast[i];
-      } else if (mode == SA_START_GIVEN) {
-        x = (double)A.v0[i];
-      } else if (mode == SA_START_DIAGONAL) {
-        const double ldi = fmax((double)A.ld[i], kLog2Clamp);
-        const T wgt = (T)exp2(0.5 * (P.alpha - P.alpha_prev) * ldi);
-        x = (double)(T)(wgt * A.ylast[i]);
-      } else {   // SECANT
-        const T yl = A.ylast[i];
-        const T yp = A.has_prev ? (T)(sgn * A.yprev[i]) : yl;
-        const T sdiff = (T)(yl - yp);
-        x = (double)(T)(yl + (T)P.secant_gamma * sdiff);
-        v[1] += (double)sdiff * (double)sdiff;
-      }
-      const T xt = (T)x;
-      A.w[i] = xt;
-      A.u[i] = A.sigma[i] * xt;
-      v[0] += (double)xt * (double)xt;
-    }
-    v[2] = v[0];
-    block_store_partials<3>(v, A.part, A.pw, 0, sm);
-    if (!grid_barrier(&C->gs, [&] {
-          reduce_partials(A.part, A.pw, gridDim.x, 3, sh);
-          if (threadIdx.x == 0) {
-            const int md = C->mode;
-            const double nrm = sqrt(sh[0]);
-            const double nin = (md == SA_START_RANDOM) ? 0.0 : (md == SA_START_SECANT ? 2.0 : 1.0);
-            C->bytes += (double)n * sizeof(T) * (2.0 + nin) + (md == SA_START_DIAGONAL ? 8.0 * n : 0.0);
-            C->action = ACT_NEXT;
-            if (md == SA_START_DIAGONAL && nrm < kTinyNorm) {
-              C->mode = SA_START_RANDOM;           // utils/predictors.py:22-25
-              C->action = ACT_P0_AGAIN;
-            } else if (md == SA_START_SECANT &&
-                       (!A.has_prev || sqrt(sh[1]) < kTinyNorm || nrm < kTinyNorm)) {
-              C->mode = SA_START_PREV;             // utils/predictors.py:44-55
-              C->action = ACT_P0_AGAIN;
-            } else if (!(nrm > 0.0) || !isfinite(nrm)) {
-              C->status = SA_ERR_NONFINITE;
-              C->action = ACT_ERROR;
-            } else {
-              C->inv_b = 1.0 / nrm;
-              C->j = 0;
-              C->pass2 = 0;
-            }
-          }
-        })) return;
-    const int act = vload(&C->action);
-    if (act == ACT_P0_AGAIN) continue;
-    if (act == ACT_ERROR) return;
-
-    // ---------------- Lanczos steps ----------------------------------------------------------
-    bool restart_p0 = false;
-    while (true) {
-      const int j = vload(&C->j);
-      const int pass2 = vload(&C->pass2);
-      if (!pass2) {
-        // P1: V[j] = w * inv_b; w <- S V[j]; partial sums of a_j = V[j] . w
-        const T inv_b = (T)vload(&C->inv_b);
-        T* Vj = A.V + (long long)j * A.ldv;
-        const T trho = (T)rho;
-        double pa[1] = {0.0};
-        spmv_items<T, RP>(A.S, A.u, gwarp, nwarps, ssp, [&](long long r, T acc) {
-          const T wr = __ldcg(A.w + r);
-          const T vr = wr * inv_b;
-          const T wn = (trho * wr - __ldcg(A.sigma + r) * acc) * inv_b;
-          Vj[r] = vr;
-          A.w[r] = wn;
-          pa[0] += (double)vr * (double)wn;
-        });
-        block_store_partials<1>(pa, A.part, A.pw, 0, sm);
-        if (!grid_barrier(&C->gs, [&] {
-              reduce_partials(A.part, A.pw, gridDim.x, 1, sm);
-              if (threadIdx.x == 0) {
-                C->a[j] = sm[0];
-                C->bytes += A.spmv_bytes + (double)n * sizeof(T);
-                C->spmvs += 1;
-              }
-            })) return;
-      }
-      // P2: three-term step w -= a_j V[j] + b_{j-1} V[j-1] (first pass only), then the
-      // reorthogonalisation coefficients h_k = V_k . w (k <= j) and ww = w . w. Removing the
-      // dominant components explicitly first keeps the single Gram-Schmidt pass stable.
-      {
-        const double a3 = pass2 ? 0.0 : vload(&C->a[j]);
-        const double b3 = (pass2 || j == 0) ? 0.0 : vload(&C->b[j - 1]);
-        const T* Vj = A.V + (long long)j * A.ldv;
-        const T* Vm = A.V + (long long)(j > 0 ? j - 1 : 0) * A.ldv;
-        for (int kb = 0; kb <= j; kb += kDotBatch) {
-          double acc[kDotBatch + 1];
-#pragma unroll
-          for (int q = 0; q <= kDotBatch; ++q) acc[q] = 0.0;
-          const int nk = (j + 1 - kb < kDotBatch) ? (j + 1 - kb) : kDotBatch;
-          for (long long i = gtid; i < n; i += nthreads) {
-            double wi = (double)__ldcg(A.w + i);
-            if (kb == 0 && !pass2) {
-              wi -= a3 * (double)__ldcg(Vj + i);
-              if (j > 0) wi -= b3 * (double)__ldcg(Vm + i);
-              const T wt = (T)wi;
-              A.w[i] = wt;
-              wi = (double)wt;
-            }
-#pragma unroll
-            for (int q = 0; q < kDotBatch; ++q)
-              if (q < nk) acc[q] += (double)__ldcg(A.V + (long long)(kb + q) * A.ldv + i) * wi;
-            if (kb == 0) acc[kDotBatch] += wi * wi;
-          }
-          block_store_partials<kDotBatch + 1>(acc, A.part, A.pw, kb * 2, sm);
-        }
-      }
-      if (!grid_barrier(&C->gs, [&] {
-            // batch kb stored its 8 dots at cols [2kb, 2kb + 8) and ww (kb = 0) at col 8
-            const int nb = (j + kDotBatch) / kDotBatch;
-            reduce_partials(A.part, A.pw, gridDim.x, 2 * kDotBatch * (nb - 1) + kDotBatch + 1, sm);
-            if (threadIdx.x <= j) {
-              const int kb = (threadIdx.x / kDotBatch) * kDotBatch;
-              C->h[threadIdx.x] = sm[2 * kb + (threadIdx.x - kb)];
-            }
-            if (threadIdx.x == 0) {
-              C->ww = sm[kDotBatch];
-              C->a[j] += sm[2 * ((j / kDotBatch) * kDotBatch) + (j % kDotBatch)];
-              C->bytes += (double)n * sizeof(T) * (double)(j + 2 + (C->pass2 ? 0 : 3));
-            }
-          })) return;
-      // P3: w -= sum_k h_k V_k ; u = sigma w ; ww2
-      {
-        if (threadIdx.x <= j) sh[threadIdx.x] = vload(&C->h[threadIdx.x]);
-        __syncthreads();
-        double v[1] = {0.0};
-        for (long long i = gtid; i < n; i += nthreads) {
-          double corr = 0.0;
-          for (int k = 0; k <= j; ++k) corr += sh[k] * (double)__ldcg(A.V + (long long)k * A.ldv + i);
-          const T wi = (T)((double)__ldcg(A.w + i) - corr);
-          A.w[i] = wi;
-          A.u[i] = A.sigma[i] * wi;
-          v[0] += (double)wi * (double)wi;
-        }
-        block_store_partials<1>(v, A.part, A.pw, 0, sm);
-      }
-      if (!grid_barrier(&C->gs, [&] {
-            reduce_partials(A.part, A.pw, gridDim.x, 1, sm);
-            const double ww2 = sm[0];
-            const double bj = sqrt(ww2);
-            const double aj = C->a[j];
-            if (threadIdx.x == 0) {
-              C->action = ACT_NEXT;
-              C->bytes += (double)n * sizeof(T) * (double)(j + 5);
-              if (!C->pass2) C->iters += 1;
-              if (!isfinite(aj) || !isfinite(bj) || fabs(aj) > bound || bj > bound) {
-                C->status = SA_ERR_BREAKDOWN;   // models/spectral_annealing.py:85-120
-                C->action = ACT_ERROR;
-              } else if (C->test_pred && j == 0) {
-                C->test_pred = 0;
-                C->pred_residual = bj;
-                C->pred_accepted = (bj > P.pred_tol) ? 0 : 1;
-                if (bj > P.pred_tol) {           // models/spectral_annealing.py:610-612
-                  C->mode = SA_START_PREV;
-                  C->iters = 0;
-                  C->action = ACT_REJECT;
-                }
-              }
-              if (C->action == ACT_NEXT && !C->pass2 && ww2 < 1e-4 * C->ww && bj > 1e-14 * bound) {
-                C->pass2 = 1;                    // second Gram-Schmidt pass
-                C->action = ACT_REPASS;
-              }
-              C->pass2 = (C->action == ACT_REPASS) ? 1 : 0;
-            }
-            __syncthreads();
-            const int act0 = C->action;
-            if (act0 == ACT_NEXT) {
-              const int m = j + 1;
-              const double th = smallest_eig_block(C->a, C->b, m);
-              if (threadIdx.x == 0) {
-                s_theta = th;
-                s_s2 = last_component_sq(C->a, C->b, m, th);
-              }
-              __syncthreads();
-              if (threadIdx.x == 0) {
-                const double res = bj * sqrt(s_s2);
-                const bool invariant = bj <= 1e-14 * bound;
-                C->theta = s_theta;
-                C->res_est = invariant ? 0.0 : res;
-                const bool conv = invariant || res <= P.tol;
-                if (conv || C->iters >= P.maxiter) {
-                  tridiag_eigvec(C->a, C->b, m, s_theta, C->s);
-                  C->status = conv ? SA_OK : SA_ERR_NOT_CONVERGED;
-                  C->b[j] = bj;
-                  C->action = ACT_DONE;
-                } else if (m >= ncv) {
-                  C->restarts += 1;
-                  C->action = ACT_RESTART;
-                } else {
-                  C->b[j] = bj;
-                  C->inv_b = 1.0 / bj;
-                  C->j = j + 1;
-                }
-              }
-              __syncthreads();
-              if (C->action == ACT_RESTART) {
-                const int kk = max(1, min(kDotBatch, ncv / 2));
-                implicit_restart(C, A.dense, A.dense + kNcvMax * kNcvMax, m, kk);
-              }
-            }
-          })) return;
-      const int act = vload(&C->action);
-      if (act == ACT_NEXT) continue;
-      if (act == ACT_REPASS) continue;
-      if (act == ACT_ERROR) return;
-      if (act == ACT_REJECT) { restart_p0 = true; break; }
-      if (act == ACT_RESTART) {
-        // kept basis V[0..kk) <- V Q[:, 0..kk) and the new residual
-        // f = V Q[:, kk] T+[kk][kk-1] + w Q[m-1][kk-1], row by row in place (all m inputs of a row
-        // are read before its kk outputs are written)
-        const int m = j + 1;
-        const int kk = vload(&C->irl_k);
-        const double beta_hat = vload(&C->irl_beta), sig_q = vload(&C->irl_sigma);
-        const double* Qd = A.dense + kNcvMax * kNcvMax;
-        for (int idx = threadIdx.x; idx < m * (kk + 1); idx += blockDim.x) {
-          const int r = idx / (kk + 1), c = idx % (kk + 1);
-          sq[idx] = vload(Qd + r * m + c);
-        }
-        __syncthreads();
-        double v[1] = {0.0};
-        for (long long i = gtid; i < n; i += nthreads) {
-          double y[kDotBatch + 1];
-#pragma unroll
-          for (int c = 0; c <= kDotBatch; ++c) y[c] = 0.0;
-          for (int r = 0; r < m; ++r) {
-            const double vr = (double)A.V[(long long)r * A.ldv + i];
-#pragma unroll
-            for (int c = 0; c <= kDotBatch; ++c)
-              if (c <= kk) y[c] += vr * sq[r * (kk + 1) + c];
-          }
-#pragma unroll
-          for (int c = 0; c < kDotBatch; ++c)
-            if (c < kk) A.V[(long long)c * A.ldv + i] = (T)y[c];
-          double yk = 0.0;
-#pragma unroll
-          for (int c = 0; c <= kDotBatch; ++c)
-            if (c == kk) yk = y[c];
-          const T f = (T)(yk * beta_hat + (double)A.w[i] * sig_q);
-          A.w[i] = f;
-          A.u[i] = A.sigma[i] * f;
-          v[0] += (double)f * (double)f;
-        }
-        block_store_partials<1>(v, A.part, A.pw, 0, sm);
-        if (!grid_barrier(&C->gs, [&] {
-              reduce_partials(A.part, A.pw, gridDim.x, 1, sm);
-              if (threadIdx.x == 0) {
-                const double nf = sqrt(sm[0]);
-                C->pass2 = 0;
-                C->bytes += (double)n * sizeof(T) * (double)(m + kk + 3);
-                if (!(nf > 1e-14 * bound) || !isfinite(nf)) {
-                  // the kept basis spans an invariant subspace: finish with its Ritz vector
-                  const double th = kth_eig(C->a, C->b, kk, 0);
-                  C->theta = th;
-                  tridiag_eigvec(C->a, C->b, kk, th, C->s);
-                  C->j = kk - 1;
-                  C->res_est = 0.0;
-                  C->status = SA_OK;
-                  C->action = ACT_DONE;
-                } else {
-                  C->b[kk - 1] = nf;
-                  C->inv_b = 1.0 / nf;
-                  C->j = kk;
-                  C->action = ACT_NEXT;
-                }
-              }
-            })) return;
-        if (vload(&C->action) == ACT_DONE) break;
-        continue;
-      }
-      break;   // ACT_DONE
-    }
-    if (restart_p0) continue;
-    break;
-  }
-
-  // ---------------- F1: Ritz vector y = V s, norm, alignment dot ------------------------------
-  const int jf = vload(&C->j);
-  if (threadIdx.x <= jf) sh[threadIdx.x] = vload(&C->s[threadIdx.x]);
-  __syncthreads();
-  {
-    double v[2] = {0.0, 0.0};
-    int bad = 0;
-    const bool align = P.align && A.has_last;
-    for (long long i = gtid; i < n; i += nthreads) {
-      double y = 0.0;
-      for (int k = 0; k <= jf; ++k) y += sh[k] * (double)__ldcg(A.V + (long long)k * A.ldv + i);
-      const T yt = (T)y;
-      if (!isfinite((double)yt)) bad = 1;
-      A.yout[i] = yt;
-      A.u[i] = A.sigma[i] * yt;
-      v[0] += (double)yt * (double)yt;
-      if (align) v[1] += (double)yt * (double)A.ylast[i];
-    }
-    if (bad) atomicOr(&C->nonfinite, 1);
-    block_store_partials<2>(v, A.part, A.pw, 0, sm);
-  }
-  if (!grid_barrier(&C->gs, [&] {
-        reduce_partials(A.part, A.pw, gridDim.x, 2, sh);
-        if (threadIdx.x == 0) {
-          const double nrm = sqrt(sh[0]);
-          const bool align = P.align && A.has_last;
-          C->nrm_y = nrm;
-          C->align_dot = align ? sh[1] : 0.0;
-          C->bytes += (double)n * sizeof(T) * (double)(jf + 3 + (align ? 1 : 0));
-          const double sg = (align && sh[1] < 0.0) ? -1.0 : 1.0;
-          C->scale = (nrm > 0.0) ? sg / nrm : sg;
-        }
-      })) return;
-
-  // ---------------- F2: true residual (one SpMV) and rounding -----------------------------------
-  const double theta = vload(&C->theta);
-  const double scale = vload(&C->scale);
-  {
-    double v[1] = {0.0};
-    if (P.residual_check) {
-      const T trho = (T)rho;
-      spmv_items<T, RP>(A.S, A.u, gwarp, nwarps, ssp, [&](long long r, T acc) {
-        const T yt = __ldcg(A.yout + r);
-        const double yr = (double)yt;
-        const double sy = (double)(trho * yt - __ldcg(A.sigma + r) * acc);
-        const double rr = sy - theta * yr;
-        v[0] += rr * rr;
-      });
-    }
-    if (P.round) {
-      const long long nr = (n + 31) & ~31ll;
-      const T ts = (T)scale;
-      unsigned long long hs = 0ull;
-      for (long long i = gtid; i < nr; i += nthreads) {
-        bool bit = false;
-        if (i < n) {
-          const T x = (T)(A.yout[i] * ts) * (T)((double)A.sigma[i] * A.sqrt_c);
-          bit = x >= T(0);
-        }
-        const unsigned int word = __ballot_sync(0xffffffffu, bit);
-        if ((threadIdx.x & 31) == 0) {
-          A.bits[i >> 5] = word;
-          hs += word_mix(i >> 5, word);
-        }
-      }
-      if ((threadIdx.x & 31) == 0 && hs) atomicAdd(&C->sig, hs);
-    }
-    block_store_partials<1>(v, A.part, A.pw, 0, sm);
-  }
-  if (!grid_barrier(&C->gs, [&] {
-        reduce_partials(A.part, A.pw, gridDim.x, 1, sh);
-        if (threadIdx.x == 0) {
-          C->rr = sh[0];
-          if (P.residual_check) { C->bytes += A.spmv_bytes; C->spmvs += 1; }
-          if (P.round) C->bytes += (double)n * sizeof(T) + (double)n / 8.0;
-          C->bytes += 2.0 * (double)n * sizeof(T);   // F3
-        }
-      })) return;
-  // F3: y <- scale * y (aligned, unit norm)
-  {
-    const T ts = (T)scale;
-    for (long long i = gtid; i < n; i += nthreads) A.yout[i] = A.yout[i] * ts;
-  }
+__global__ void __launch_bounds__(kThreads, 1) alpha_kernel(AlphaArgs<T, RP> A) {
+  alpha_body<T, RP>(A, GridPolicy{});
 }
 
 // ---- host side ------------------------------------------------------------------------------

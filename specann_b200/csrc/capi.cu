@@ -136,7 +136,7 @@ __global__ void scale_kernel(const double* ld, long long n, double alpha, double
 }
 
 template <typename T, typename RP>
-__global__ void __launch_bounds__(kThreads, 3) spmv_kernel(SpmvArgs<T, RP> S, int group, const T* u, const T* x,
+__global__ void __launch_bounds__(kThreads, 2) spmv_kernel(SpmvArgs<T, RP> S, int group, const T* u, const T* x,
                                                          const T* sigma, T rho, T* y) {
   __shared__ SpmvSmem<T> ssp;
   const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -219,7 +219,8 @@ void build_items(const std::vector<long long>& rp, long long n, std::vector<Work
   long long part = 0, seg_begin = -1, seg_rows = 0, seg_elems = 0;
   long long short_rows = 0, short_elems = 0;
   auto flush = [&](long long end) {
-    if (seg_begin >= 0) items.push_back(WorkItem{seg_begin, (int)end, -1});
+    if (seg_begin >= 0)
+      items.push_back(WorkItem{rp[seg_begin], (int)seg_begin, (int)((rp[end] - rp[seg_begin]) | ((end - seg_begin) << 9))});
     seg_begin = -1;
     seg_rows = 0;
     seg_elems = 0;
@@ -229,13 +230,15 @@ void build_items(const std::vector<long long>& rp, long long n, std::vector<Work
     if (d > kShortMax) {
       flush(r);
       const long long nch = (d + kChunk - 1) / kChunk;
-      if (nch == 1) {
-        items.push_back(WorkItem{-(r + 1), 0, -1});
-      } else {
-        const int z = (int)mc_base.size();
+      int zcode = 0;
+      if (nch > 1) {
+        zcode = (int)mc_base.size() + 1;
         mc_base.push_back(part);
         part += nch;
-        for (long long c = 0; c < nch; ++c) items.push_back(WorkItem{-(r + 1), (int)c, z});
+      }
+      for (long long c = 0; c < nch; ++c) {
+        const long long len = std::min<long long>(kChunk, d - c * kChunk);
+        items.push_back(WorkItem{rp[r] + c * kChunk, (int)(-(r + 1)), (int)(len | ((long long)zcode << 9))});
       }
     } else {
       if (seg_begin >= 0 && seg_elems + d > kSegMax) flush(r);
@@ -427,7 +430,7 @@ int sa_spmv_scaled(sa_handle* h, double alpha, double rho, const void* x, void* 
   if (!h || !h->bound || !x || !y) return SA_ERR_INVALID_ARG;
   const int g = grid_for(h->n, 256, h->sm_count);
   const double hl = 0.5 * std::log2(h->c);
-  const int gs = h->sm_count * 3;
+  const int gs = h->sm_count * 2;
   if (h->n_mc) SA_CUDA(cudaMemsetAsync(h->mc_count, 0, 4 * h->n_mc, h->stream));
   if (h->prec == 32) {
     scale_kernel<float><<<g, 256, 0, h->stream>>>(h->ld, h->n, alpha, hl, (const float*)x, (float*)h->sigma, (float*)h->u);
@@ -493,6 +496,7 @@ int sa_alpha_solve(sa_handle* h, const sa_alpha_params* p, sa_alpha_record* rec)
   rec->basis_used = ctl.j + 1;
   rec->spmv_count = ctl.spmvs;
   rec->alg_bytes = ctl.bytes;
+  for (int q = 0; q < 6; ++q) rec->phase_ms[q] = (double)ctl.tph[q] * 1e-6;
   if (rec->status != SA_OK && std::getenv("SPECANN_DEBUG")) {
     std::fprintf(stderr, "[specann] alpha_solve status %d: j=%d iters=%d restarts=%d action=%d theta=%.17g ww=%.6g inv_b=%.6g\n",
                  rec->status, ctl.j, ctl.iters, ctl.restarts, ctl.action, ctl.theta, ctl.ww, ctl.inv_b);

@@ -18,14 +18,19 @@ constexpr int kNcvMax = 64;               // largest Lanczos basis
 constexpr int kDotBatch = 8;              // basis vectors per register batch in the dot phase
 constexpr unsigned long long kSpinLimit = 1ull << 25;   // ~2 s of 64 ns sleeps
 
-// One entry of the SpMV work list. Short segment: x = first row (>= 0), y = end row,
-// z = unused. Long-row chunk: x = -(row + 1), y = chunk index, z = multi-chunk row id (-1 when
-// the row fits in one chunk).
+// One tile of the SpMV work list: at most kSegMax stored entries starting at e0.
+//   row >= 0: a short segment of rows [row, row + nrows);
+//   row < 0:  a chunk of the long row -(row + 1).
+//   meta bits 0-8: entries in the tile; segment: bits 9-15 nrows; chunk: bits 9-31 hold
+//   (multi-chunk row id + 1), 0 when the row fits in one chunk.
 struct WorkItem {
-  long long x;
-  int y;
-  int z;
+  long long e0;
+  int row;
+  int meta;
 };
+__host__ __device__ __forceinline__ int item_len(int meta) { return meta & 511; }
+__host__ __device__ __forceinline__ int item_nrows(int meta) { return (meta >> 9) & 127; }
+__host__ __device__ __forceinline__ int item_mc(int meta) { return (int)((unsigned)meta >> 9) - 1; }
 
 // Device-resident synchronisation block of a persistent kernel (zeroed before launch).
 struct GridSync {

@@ -43,6 +43,7 @@ struct AlphaCtrl {
   int irl_k;                // basis vectors kept by the last implicit restart
   double irl_beta;          // T+[k][k-1] of the last implicit restart
   double irl_sigma;         // Q[m-1][k-1] of the last implicit restart
+  unsigned long long tph[6];  // ns by phase (set-up, SpMV, dots, update+Ritz, restart, final)
 };
 
 // Control block of the local-search kernel.

@@ -2,25 +2,27 @@
 // the residual check.
 //
 // The rows are cut once per matrix (sa_set_matrix) into a work list in row order whose items are
-// warp tiles of at most kSegMax = 256 entries:
+// warp tiles of at most kSegMax = 256 stored entries (start offset and length stored in the item):
 //   * short segments: runs of consecutive rows with at most kShortMax entries each (at most
-//     kSegRows rows, at most kSegMax entries);
+//     kSegRows rows);
 //   * long-row chunks: rows with more than kShortMax entries cut into chunks of kChunk entries.
-// A warp streams its tile's columns and values with kTileIt fully coalesced, independent loads per
-// lane (lane l takes entries l, l + 32, ...), issues the kTileIt gathers of u, and multiplies. For
-// a segment the products go to a per-warp shared buffer and one lane per row adds its contiguous
-// range in order; for a chunk the lanes' partial sums are combined by a fixed xor-shuffle tree.
-// A row of one chunk is finished by its warp. For a row of several chunks every warp stores its
-// partial sum and the warp that finishes last (an atomic ticket per row) adds the partials in chunk
-// order and finishes the row. No spin-waits, and no summation order depends on timing.
+// A warp streams a tile's columns and values with kTileIt fully coalesced, independent loads per
+// lane (lane l takes entries l, l + 32, ...), gathers u and multiplies. For a segment the products
+// go to a per-warp shared buffer and one lane per row adds its contiguous range in order; for a
+// chunk the lanes' partial sums are combined by a fixed xor-shuffle tree. A row of one chunk is
+// finished by its warp. For a row of several chunks every warp stores its partial sum and the warp
+// that finishes last (an atomic ticket per row) adds the partials in chunk order and finishes the
+// row. No spin-waits, and no summation order depends on timing.
 //
 // Warps take items round robin (item t -> warp t mod warps), so concurrent warps stream
-// neighbouring parts of col/val. col, val, rowptr and the work list are read through the
-// read-only path. The gathered vector u is read through the read-only path too when it is
-// immutable for the whole kernel (kReadOnlyU, the standalone operator); the persistent kernels
-// rewrite u between phases, so there it is read with ordinary L1-allocating loads, which see the
-// writes of other CTAs because every phase boundary is a grid barrier (gpu-scope fence by the
-// waiting thread, then bar.sync).
+// neighbouring parts of col/val. Each warp runs a three-stage software pipeline: the descriptor of
+// the tile after next and the columns/values of the next tile are in flight while the current
+// tile's gathers and row sums run, so the HBM stream overlaps the gather latency.
+// col, val, rowptr and the work list are read through the read-only path. The gathered vector u
+// is read through the read-only path too when it is immutable for the whole kernel (kReadOnlyU,
+// the standalone operator); the persistent kernels rewrite u between phases, so there it is read
+// with ordinary L1-allocating loads, which see the writes of other CTAs because every phase
+// boundary is a grid barrier (gpu-scope fence by the waiting thread, then bar.sync).
 #pragma once
 #include "common.cuh"
 
@@ -45,13 +47,45 @@ struct SpmvSmem {
   int rp[kWarps][kSegRows + 1];
 };
 
-// fin(row, sum) is called exactly once per row with sum = sum_j val_ij * u_j (T arithmetic).
 template <bool kReadOnlyU, typename T>
 __device__ __forceinline__ T gather(const T* u, int j) {
   if (kReadOnlyU) return __ldg(u + j);
   return u[j];
 }
 
+struct TileDesc {
+  long long e0;
+  int row;
+  int meta;
+};
+
+__device__ __forceinline__ TileDesc load_desc(const WorkItem* items, long long t, long long n_items) {
+  TileDesc d{0, 0, 0};
+  if (t < n_items) {
+    d.e0 = __ldg(&items[t].e0);
+    d.row = __ldg(&items[t].row);
+    d.meta = __ldg(&items[t].meta);
+  }
+  return d;
+}
+
+template <typename T>
+__device__ __forceinline__ void load_tile(const int* col, const T* val, const TileDesc& d, int lane,
+                                          int (&ci)[kTileIt], T (&v)[kTileIt]) {
+  const int len = item_len(d.meta);
+#pragma unroll
+  for (int q = 0; q < kTileIt; ++q) {
+    const int k = lane + 32 * q;
+    ci[q] = 0;
+    v[q] = T(0);
+    if (k < len) {
+      ci[q] = __ldg(col + d.e0 + k);
+      v[q] = __ldg(val + d.e0 + k);
+    }
+  }
+}
+
+// fin(row, sum) is called exactly once per row with sum = sum_j val_ij * u_j (T arithmetic).
 template <typename T, typename RP, bool kReadOnlyU = false, class Fin>
 __device__ __forceinline__ void spmv_items(const SpmvArgs<T, RP>& S, const T* u, long long gwarp,
                                            long long nwarps, SpmvSmem<T>& sm, Fin&& fin) {
@@ -59,42 +93,28 @@ __device__ __forceinline__ void spmv_items(const SpmvArgs<T, RP>& S, const T* u,
   const int wid = threadIdx.x >> 5;
   T* prod = sm.prod[wid];
   int* srp = sm.rp[wid];
-  for (long long it = gwarp; it < S.n_items; it += nwarps) {
-    const long long ix = __ldg(&S.items[it].x);
-    const int iy = __ldg(&S.items[it].y);
-    long long e0, e1, row = 0;
-    int z = -1;
-    if (ix >= 0) {
-      e0 = rp_load(S.rowptr, ix);
-      e1 = rp_load(S.rowptr, iy);
-    } else {
-      row = -(ix + 1);
-      z = __ldg(&S.items[it].z);
-      const long long rs = rp_load(S.rowptr, row), re = rp_load(S.rowptr, row + 1);
-      e0 = rs + (long long)iy * kChunk;
-      e1 = (e0 + kChunk < re) ? e0 + kChunk : re;
-    }
-    const int len = (int)(e1 - e0);
-    int ci[kTileIt];
-    T v[kTileIt];
-#pragma unroll
-    for (int q = 0; q < kTileIt; ++q) {
-      const int k = lane + 32 * q;
-      ci[q] = 0;
-      v[q] = T(0);
-      if (k < len) {
-        ci[q] = __ldg(S.col + e0 + k);
-        v[q] = __ldg(S.val + e0 + k);
-      }
-    }
+  long long it = gwarp;
+  TileDesc cur = load_desc(S.items, it, S.n_items);
+  int ci[kTileIt];
+  T v[kTileIt];
+  load_tile(S.col, S.val, cur, lane, ci, v);
+  TileDesc nxt = load_desc(S.items, it + nwarps, S.n_items);
+  while (it < S.n_items) {
+    // stage 1: next tile's entries and the descriptor after it are put in flight
+    int cn[kTileIt];
+    T vn[kTileIt];
+    load_tile(S.col, S.val, nxt, lane, cn, vn);
+    const TileDesc nn = load_desc(S.items, it + 2 * nwarps, S.n_items);
+    // stage 2: the current tile
+    const int len = item_len(cur.meta);
 #pragma unroll
     for (int q = 0; q < kTileIt; ++q) {
       const int k = lane + 32 * q;
       if (k < len) v[q] *= gather<kReadOnlyU>(u, ci[q]);
     }
-    if (ix >= 0) {
-      const int nr = iy - (int)ix;
-      for (int k = lane; k <= nr; k += 32) srp[k] = (int)(rp_load(S.rowptr, ix + k) - e0);
+    if (cur.row >= 0) {
+      const int nr = item_nrows(cur.meta);
+      for (int k = lane; k <= nr; k += 32) srp[k] = (int)(rp_load(S.rowptr, cur.row + k) - cur.e0);
 #pragma unroll
       for (int q = 0; q < kTileIt; ++q) {
         const int k = lane + 32 * q;
@@ -105,10 +125,12 @@ __device__ __forceinline__ void spmv_items(const SpmvArgs<T, RP>& S, const T* u,
         const int b = srp[r], e = srp[r + 1];
         T acc = T(0);
         for (int q = b; q < e; ++q) acc += prod[q];
-        fin(ix + r, acc);
+        fin((long long)cur.row + r, acc);
       }
       __syncwarp();
     } else {
+      const long long row = -((long long)cur.row + 1);
+      const int z = item_mc(cur.meta);
       T acc = T(0);
 #pragma unroll
       for (int q = 0; q < kTileIt; ++q) acc += v[q];
@@ -120,7 +142,8 @@ __device__ __forceinline__ void spmv_items(const SpmvArgs<T, RP>& S, const T* u,
           const long long rs = rp_load(S.rowptr, row), re = rp_load(S.rowptr, row + 1);
           const long long base = __ldg(S.mc_base + z);
           const int nch = (int)((re - rs + kChunk - 1) / kChunk);
-          S.long_part[base + iy] = acc;
+          const int chunk = (int)((cur.e0 - rs) / kChunk);
+          S.long_part[base + chunk] = acc;
           __threadfence();
           const int ticket = atomicAdd(S.mc_count + z, 1);
           if (ticket == nch - 1) {
@@ -133,6 +156,15 @@ __device__ __forceinline__ void spmv_items(const SpmvArgs<T, RP>& S, const T* u,
         }
       }
     }
+    // rotate the pipeline
+    cur = nxt;
+    nxt = nn;
+#pragma unroll
+    for (int q = 0; q < kTileIt; ++q) {
+      ci[q] = cn[q];
+      v[q] = vn[q];
+    }
+    it += nwarps;
   }
 }
 

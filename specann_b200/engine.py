@@ -129,6 +129,9 @@ class Engine:
             self.stats["alpha_bytes"] += rec.alg_bytes
             self.stats["alpha_launches"] += 1
             self.stats["spmvs"] += rec.spmv_count
+            ph = self.stats.setdefault("phase_ms", [0.0] * 6)
+            for q in range(6):
+                ph[q] += rec.phase_ms[q]
         return rec
 
     def result_vector(self) -> torch.Tensor:

@@ -311,6 +311,7 @@ class SpectralAnnealing:
                 'pred_residual': pred_rec.pred_residual, 'pred_accepted': pred_acc,
                 'candidate': slot if self.use_local_search else None,
                 'eigsh_residual': rec.residual, 'eigsh_restarts': int(rec.restarts),
+                'eigsh_spmvs': int(rec.spmv_count), 'alg_bytes': float(rec.alg_bytes),
                 'timestamp': datetime.now().strftime('%Y-%m-%d %H:%M:%S')})
             row_cand.append(slot)
         sweep_end = time.time()

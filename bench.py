@@ -45,6 +45,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-alphas", type=int, default=2)
     ap.add_argument("--spmv-reps", type=int, default=20)
+    ap.add_argument("--workload", default="metric", choices=["metric", "batch", "precision", "grad"],
+                    help="metric: the headline solve (default); batch: the ragged batched workload "
+                         "(64 instances x 4 seeds x 128 alphas, one launch); precision: FP32 + FP64 Ritz vs "
+                         "all-FP64 on BA(2^16); grad: the differentiation workload on BA(2^18)")
     ap.add_argument("--scale-run", action="store_true",
                     help="one timed FP32 solve and one timed plain-FP64 solve of the graph, with the energy gap")
     ap.add_argument("--spmv-only", action="store_true",
@@ -170,6 +174,174 @@ def cpu_baseline_sample(args, n, rowptr, col, val):
                       f"({dt:.1f} s measured), x{scale:g}; SciPy ARPACK eigsh and NumPy, single-threaded"}
 
 
+def run_batch(args, rank, world, local):
+    """The ragged batched workload: 64 instances (n log-uniform in [2^10, 2^17], half ER degree 20,
+    half BA m 10/20, +-1 couplings) x 4 seeds x 128 alphas in one launch per GPU. Under torchrun the
+    instances are sharded over the ranks (strong scaling: the total work is fixed); the time is the
+    max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from specann_b200 import _lib, graphs, sharding
+    from specann_b200.batch import BatchedSpectralAnnealing
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    lib = _lib.load()
+    inst = graphs.ragged_batch()
+    Js = [J for _, J in inst]
+    seeds = (42, 43, 44, 45)
+    mine = sharding.shard_instances([(J.shape[0], J.nnz) for J in Js], world)[rank]
+    mJs = [Js[i] for i in mine]
+    b = BatchedSpectralAnnealing(seeds=seeds, num_alphas=args.num_alphas)
+    b.load(mJs)
+    tune = b.autotune(splits=(1.0, 2.0, 4.0), num_alphas=8)
+    for _ in range(args.warmup):
+        b.sweep()
+    clocks = ClockSampler(local)
+    launches0 = lib.sa_kernel_launches()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    times = [b.sweep() for _ in range(args.steps)]
+    clk = clocks.stop()
+    launches = lib.sa_kernel_launches() - launches0
+    ms = float(np.mean(times))
+    res = b.results()
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    spmvs = sum(r2["eigsh_spmvs"] for r in res for r2 in r["rows"])
+    alg = 0.0
+    for r in res:
+        J = mJs[r["instance"]]
+        per = J.nnz * 8 + (J.shape[0] + 1) * 4 + 12 * J.shape[0]
+        alg += per * sum(x["eigsh_spmvs"] for x in r["rows"])
+    hbm, kind = peaks()
+    # e2e: host CSRs -> upload + preludes -> batched launch -> best spins back, through the public API
+    t0 = time.perf_counter()
+    e2 = BatchedSpectralAnnealing(seeds=seeds, num_alphas=args.num_alphas, split=b._built_split)
+    out = e2.solve(mJs)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2.close()
+    if world > 1:
+        tt = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    h2d = int(sum(J.indptr.size * 4 + J.nnz * 8 for J in mJs))
+    d2h = int(sum(J.shape[0] for J in mJs) * len(seeds) // 8)
+    line = {"metric": "s per ragged batch (64 instances x 4 seeds x 128 alphas, one launch per GPU)",
+            "value": ms / 1000.0, "unit": "s/batch", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded ER/BA generators, +-1 couplings)",
+            "config": {"workload": "ragged batch: 64 instances, n log-uniform 2^10..2^17, half ER deg 20, half BA "
+                                   "m 10/20, 4 seeds x 128 alphas sqrt, diagonal predictor, batched LS",
+                       "instances_on_rank0": len(mJs), "problems": len(mJs) * len(seeds),
+                       "total_nnz": int(sum(J.nnz for J in Js)), "teams": int(len(b.team_b0)),
+                       "largest_team": int(b.team_nb.max()), "grid": b.grid(), "autotune_ms": tune,
+                       "split": b._built_split, "graph": True,
+                       "l2": "working set of the batch (CSR + bases) larger than L2"},
+            "e2e": {"value": e2e_s, "unit": "s/batch", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": alg / (ms / 1e3) / 1e9 / hbm, "traffic": None, "peak_source": kind,
+                         "kernel": "batch_kernel (SpMV bytes only: a lower bound of its traffic)",
+                         "spmvs": spmvs},
+            "problems_ok": int(sum(1 for r in res if r["status"] == 0)),
+            "problem_device_ms": {"max": float(max(r["device_ms"] for r in res)),
+                                  "sum": float(sum(r["device_ms"] for r in res))},
+            "clocks": clk, "gpu_launches": int(launches)}
+    if rank == 0:
+        print(json.dumps(line))
+    b.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_precision(args):
+    """Precision form on BA(2^16, m 20), J = -A: FP32 SpMV/Lanczos with FP64 Ritz and residual
+    against the all-FP64 path, per alpha (eigenvalue error, residual, raw energy) and best energy."""
+    from specann_b200 import graphs
+    from specann_b200.spectral_annealing import SpectralAnnealing
+    J = graphs.barabasi_albert(1 << 16, 20, seed=42)
+    runs = {}
+    for prec in (32, 64):
+        s = SpectralAnnealing("c2.txt", "c2", random_seed=42, precision=prec, write_results=False, profile=True)
+        t0 = time.perf_counter()
+        e, spins, _ = s.solve(J)
+        dt = time.perf_counter() - t0
+        runs[prec] = (s, e, dt)
+    r32, r64 = runs[32][0].alpha_results, runs[64][0].alpha_results
+    lam_err = np.array([abs(a["lambda1"] - b["lambda1"]) for a, b in zip(r32, r64)])
+    res32 = np.array([a["eigsh_residual"] for a in r32])
+    res64 = np.array([b["eigsh_residual"] for b in r64])
+    raw_gap = np.array([abs(a["raw_energy"] - b["raw_energy"]) / abs(b["raw_energy"]) for a, b in zip(r32, r64)])
+    same = sum(1 for a, b in zip(r32, r64) if a["raw_energy"] == b["raw_energy"])
+    out = {"workload": "precision: BA(2^16, m=20) J=-A, 128 alphas sqrt, seed 42",
+           "fp32_s": runs[32][2], "fp64_s": runs[64][2], "best_fp32": runs[32][1], "best_fp64": runs[64][1],
+           "best_gap_rel": abs(runs[32][1] - runs[64][1]) / abs(runs[64][1]),
+           "lambda_abs_err": {"max": float(lam_err.max()), "median": float(np.median(lam_err))},
+           "residual_fp32": {"max": float(np.nanmax(res32)), "median": float(np.nanmedian(res32))},
+           "residual_fp64": {"max": float(np.nanmax(res64)), "median": float(np.nanmedian(res64))},
+           "raw_energy_gap_rel": {"max": float(raw_gap.max()), "median": float(np.median(raw_gap))},
+           "alphas_same_raw_energy": same, "spmvs_fp32": runs[32][0].engine.stats["spmvs"],
+           "spmvs_fp64": runs[64][0].engine.stats["spmvs"],
+           "per_alpha": [{"alpha": a["alpha"], "lambda_fp32": a["lambda1"], "lambda_fp64": b["lambda1"],
+                          "res_fp32": a["eigsh_residual"], "res_fp64": b["eigsh_residual"],
+                          "raw_fp32": a["raw_energy"], "raw_fp64": b["raw_energy"]} for a, b in zip(r32, r64)]}
+    print(json.dumps(out))
+
+
+def run_grad(args):
+    """Differentiation form on BA(2^18, m 20), +-1 couplings, beta 8: adjoint gradient time and its
+    central-FD check (h 1e-4, FP64), and Lanczos work per alpha of the three predictors."""
+    import torch
+    from specann_b200 import _lib, graphs
+    from specann_b200.differentiation import EigenProblem
+    from specann_b200.spectral_annealing import SpectralAnnealing
+    J = graphs.barabasi_albert(1 << 18, 20, seed=42, couplings="pm1")
+    out = {"workload": "grad: BA(2^18, m=20) +-1 couplings, beta 8"}
+    for prec, tol, atol in ((32, 1e-6, 1e-4), (64, 1e-10, 1e-8)):
+        prob = EigenProblem(J, precision=prec)
+        prob.energy_and_gradient(0.5, beta=8.0, tol=tol, adj_tol=atol)        # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        lam, y = prob.eigenpair(0.5, tol=tol)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        grad = torch.empty(prob.n, dtype=torch.float64, device="cuda")
+        res = prob.engine.adjoint(_lib.SA_ADJ_GRADIENT, alpha=0.5, lambda1=lam, y=y, beta=8.0, tol=atol, maxiter=4000, grad=grad)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        d = {"eig_s": t1 - t0, "adjoint_s": t2 - t1, "minres_iterations": res.iterations,
+             "minres_residual": res.residual, "loss": res.loss, "dL_dalpha": res.dloss_dalpha}
+        if prec == 64:
+            h = 1e-4
+            Lp = prob.energy_and_gradient(0.5 + h, beta=8.0, tol=tol, adj_tol=1e-2)[0]
+            Lm = prob.energy_and_gradient(0.5 - h, beta=8.0, tol=tol, adj_tol=1e-2)[0]
+            d["fd"] = (Lp - Lm) / (2 * h)
+            d["fd_rel_err"] = abs(d["fd"] - res.dloss_dalpha) / abs(d["fd"])
+        out[f"fp{prec}"] = d
+        prob.close()
+    pred = {}
+    for mode in ("diagonal", "secant", "tangent"):
+        s = SpectralAnnealing("c4.txt", "c4", random_seed=42, pred_mode=mode, write_results=False,
+                              use_local_search=False)
+        t0 = time.perf_counter()
+        e, _, _ = s.solve(J)
+        dt = time.perf_counter() - t0
+        rows = s.alpha_results
+        it = np.array([r["eigsh_iterations"] for r in rows])
+        pred[mode] = {"s": dt, "best_raw_energy": e, "lanczos_iters_mean": float(it.mean()),
+                      "lanczos_iters_median": float(np.median(it)), "lanczos_spmvs": int(sum(r["eigsh_spmvs"] for r in rows)),
+                      "tangent_spmvs": int(sum(r.get("tangent_spmvs", 0) for r in rows)),
+                      "pred_accepted": int(sum(1 for r in rows if r["pred_accepted"]))}
+    out["predictors"] = pred
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -177,6 +349,15 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "batch":
+        run_batch(args, rank, world, local)
+        return
+    if args.workload == "precision":
+        run_precision(args)
+        return
+    if args.workload == "grad":
+        run_grad(args)
         return
     import torch
     import torch.distributed as dist

@@ -37,7 +37,10 @@ typedef enum {
   SA_START_PREV = 1,       /* the previous eigenvector y_last as is (pred_mode "prev") */
   SA_START_DIAGONAL = 2,   /* utils/predictors.py:6-26, then the residual acceptance test */
   SA_START_SECANT = 3,     /* utils/predictors.py:29-56, then the residual acceptance test */
-  SA_START_GIVEN = 4       /* the device vector passed in sa_alpha_params.v0 */
+  SA_START_GIVEN = 4,      /* the device vector passed in sa_alpha_params.v0 */
+  SA_START_TANGENT = 5     /* y_last + (alpha - alpha_prev) v0 with v0 the eigenvector tangent dy/dalpha
+                              at alpha_prev (sa_adjoint, SA_ADJ_TANGENT), then the residual acceptance test; no
+                              counterpart in the reference (a third predictor beside diagonal/secant) */
 } sa_start_mode;
 
 typedef struct sa_handle sa_handle;
@@ -56,7 +59,7 @@ typedef struct {
   int32_t align;         /* 1: sign-align the result with y_last (when a y_last exists) */
   uint64_t seed;         /* seed of the random start stream */
   int64_t stream_id;     /* random stream id (alpha index and attempt) */
-  const void* v0;        /* device start vector for SA_START_GIVEN (else NULL) */
+  const void* v0;        /* device start vector (SA_START_GIVEN) or tangent (SA_START_TANGENT), else NULL */
   int32_t round;         /* 1: round x = D^{-1/2} y to packed spins and hash them */
   int32_t residual_check;/* 1: true residual ||S y - mu y|| with one more SpMV */
 } sa_alpha_params;
@@ -175,6 +178,135 @@ int sa_local_search(sa_handle* h, const sa_ls_params* p, void* ls_workspace, siz
 /* Energies E = -1/2 s^T J s of candidate slots 0..k-1 (no local search): _batch_energies /
  * fp32_energies, models/spectral_annealing.py:693-707, :962-976. */
 int sa_energies(sa_handle* h, int32_t k, void* ls_workspace, size_t ls_bytes, double* energies);
+
+/* ---- differentiation form: adjoint of the leading eigenvector ------------------------------------
+ * No counterpart in the reference (it has no gradients). With per-vertex exponents a (a_i = alpha +
+ * offset_i, offsets optional) the solves use N_a = D_a^{-1/2} (J/c) D_a^{-1/2}; the rounding vector
+ * is x = D_a^{-1/2} y (models/spectral_annealing.py:663, :345) and the smoothed energy is
+ * L = -1/2 tanh(beta x)^T J tanh(beta x). */
+
+/* Per-vertex exponent offsets used by the following sa_alpha_solve and sa_adjoint calls (device
+ * array of n doubles owned by the caller; NULL clears them). sa_spmv_scaled ignores them. */
+int sa_set_exponent_offsets(sa_handle* h, const double* offsets_device);
+
+typedef enum {
+  SA_ADJ_GRADIENT = 0,   /* dL/da per vertex (and dL/dalpha = its sum) at the eigenpair (lambda1, y) */
+  SA_ADJ_TANGENT = 1,    /* dy/dalpha at the eigenpair: the tangent predictor's direction */
+  SA_ADJ_SOLVE = 2       /* (lambda1 I - N_a) out = (I - y y^T) rhs with out orthogonal to y */
+} sa_adjoint_mode;
+
+typedef struct {
+  double alpha;          /* exponent of the eigenpair */
+  double lambda1;        /* its leading eigenvalue */
+  double beta;           /* tanh sharpness (SA_ADJ_GRADIENT) */
+  double tol;            /* MINRES tolerance on the residual relative to the right-hand side */
+  int32_t maxiter;       /* MINRES iterations at most */
+  int32_t mode;          /* sa_adjoint_mode */
+  const void* y;         /* unit leading eigenvector (device, the handle's precision) */
+  const void* rhs;       /* SA_ADJ_SOLVE: right-hand side (device) */
+  void* out;             /* SA_ADJ_TANGENT / SA_ADJ_SOLVE: the solution (device, n values) */
+  double* grad;          /* SA_ADJ_GRADIENT: dL/da_i (device, n doubles) */
+} sa_adjoint_params;
+
+typedef struct {
+  int32_t status;        /* SA_OK (tol reached, or the residual stalled below 1e-3 of the right-hand
+                            side: the eigenpair's own error bounds what the solve can resolve),
+                            SA_ERR_NOT_CONVERGED, SA_ERR_NONFINITE, ... */
+  int32_t iterations;    /* MINRES iterations */
+  int32_t spmv_count;    /* fused SpMVs of the call */
+  int32_t reserved;
+  double residual;       /* MINRES residual estimate relative to the projected right-hand side */
+  double loss;           /* SA_ADJ_GRADIENT: L at the eigenpair */
+  double dloss_dalpha;   /* SA_ADJ_GRADIENT: dL/dalpha = sum_i dL/da_i */
+} sa_adjoint_result;
+
+int sa_adjoint_workspace_size(sa_handle* h, size_t* bytes);
+
+/* One persistent cooperative launch: right-hand side, MINRES on the projected operator (FP64
+ * scalars and inner products), and for the gradient the products M w, M y and the assembly. */
+int sa_adjoint(sa_handle* h, const sa_adjoint_params* p, void* work, size_t bytes, sa_adjoint_result* res);
+
+/* ---- batched sweeps: many (instance, seed) problems in one launch ------------------------------
+ * Replaces the reference's driver loop that builds one solver per (instance, seed) and calls
+ * solve(J) on it (utils/core.py:103-105, models/spectral_annealing.py:262-525 per problem): every
+ * problem runs the whole alpha sweep (shift, start mode, alpha solve, cold retry, checks,
+ * deduplication, warm-start commit) and the local search of its distinct candidates inside one
+ * persistent cooperative kernel. Instances are sa_handle objects with a bound matrix (their prelude
+ * is reused); all must share the precision and use 32-bit row pointers. Problem p is instance
+ * p / seeds_per_instance with seed seeds[p]. */
+typedef struct sa_batch sa_batch;
+
+typedef struct {
+  double eigsh_tol, pred_tol, shift_eps, secant_gamma;
+  double subset_fraction, final_sweep_fraction;
+  int32_t num_alphas;            /* <= 128 and <= the batch's candidate capacity */
+  int32_t maxiter;
+  int32_t ncv;                   /* 0: min(33, n - 1) per instance */
+  int32_t pred_mode;             /* SA_START_DIAGONAL, SA_START_SECANT or SA_START_PREV */
+  int32_t warm_start;
+  int32_t residual_check;
+  int32_t use_local_search;
+  int32_t max_local_iterations;
+  int32_t final_sweep_iters;
+  int32_t num_rounds;
+  int32_t ls_semantics;          /* 0 priority, 1 snapshot */
+  int32_t reserved;
+} sa_batch_config;
+
+/* One alpha of one problem: the columns of the reference's per-alpha rows. */
+typedef struct {
+  double alpha, lambda1, rho, gershgorin, residual, pred_residual, degree_scale;
+  uint64_t signature;
+  int32_t status, iterations, restarts, spmv_count;
+  int32_t pred_accepted;         /* -1: no predictor test */
+  int32_t retry, converged;
+  int32_t candidate;             /* -1: the alpha was skipped */
+} sa_batch_alpha_record;
+
+/* One problem after the sweep. */
+typedef struct {
+  int32_t status, num_candidates, ls_iterations, ls_final_passes;
+  int32_t alphas_skipped, alphas_retried, team_first_block, team_blocks;
+  int32_t integer_gains, reserved;
+  int64_t ls_total_flips;
+  double device_ms;
+  double energy_before[128];     /* per candidate slot, exact integers for integer couplings */
+  double energy_after[128];
+} sa_batch_summary;
+
+/* CTAs of the batch kernel that fit on this device at once (the grid of every batch launch). */
+int sa_batch_grid(int32_t precision, int32_t rowptr64, int32_t* blocks);
+
+/* Host-only plan of problems onto teams of CTAs: the problems (sizes n, nnz) sorted by a cost
+ * model, each large one given its own team of about split x its share of `blocks` CTAs, the rest
+ * placed longest-first on the team that finishes first (barrier_cost: relative overhead of a
+ * multi-CTA team). Outputs team_of[n_prob] and the contiguous teams [team_b0, team_b0 + team_nb)
+ * (arrays of `blocks` entries; *n_teams used). No counterpart in the reference. */
+int sa_batch_plan(int32_t n_prob, const int64_t* n, const int64_t* nnz, int32_t blocks, double split,
+                  double barrier_cost, int32_t* team_of, int32_t* team_b0, int32_t* team_nb,
+                  int32_t* n_teams);
+
+int sa_batch_workspace_size(int32_t n_inst, sa_handle* const* inst, int32_t seeds_per_instance,
+                            int32_t ncv_max, int32_t capacity, int32_t n_teams, const int32_t* team_b0,
+                            const int32_t* team_nb, const int32_t* team_of, size_t* bytes);
+
+int sa_batch_create(sa_batch** out, int32_t n_inst, sa_handle* const* inst, int32_t seeds_per_instance,
+                    const uint64_t* seeds, int32_t ncv_max, int32_t capacity, int32_t n_teams,
+                    const int32_t* team_b0, const int32_t* team_nb, const int32_t* team_of,
+                    void* workspace, size_t bytes, void* stream);
+
+/* Run every problem's sweep (alphas: host array of cfg->num_alphas values). With use_graph the
+ * first call captures the launch (barrier reset + cooperative kernel) into a CUDA graph and later
+ * calls replay it. Asynchronous on the batch's stream. */
+int sa_batch_sweep(sa_batch* b, const sa_batch_config* cfg, const double* alphas, int32_t use_graph);
+
+/* Per-problem results (host arrays: records n_prob x 128, summaries n_prob); synchronises. */
+int sa_batch_results(sa_batch* b, sa_batch_alpha_record* records, sa_batch_summary* summaries);
+
+/* Packed words of candidate slot of a problem (refined: after the local search). */
+int sa_batch_candidate(sa_batch* b, int32_t problem, int32_t slot, int32_t refined, uint32_t* packed_device);
+
+int sa_batch_destroy(sa_batch* b);
 
 /* ---- allocation-free operator ------------------------------------------------------------- */
 

@@ -26,7 +26,8 @@ SA_ERR_BARRIER_TIMEOUT = 7
 STATUS_NAMES = {0: "OK", 1: "BREAKDOWN", 2: "NONFINITE", 3: "NOT_CONVERGED", 4: "OOM", 5: "INVALID_ARG",
                 6: "CUDA_ERROR", 7: "BARRIER_TIMEOUT"}
 
-SA_START_RANDOM, SA_START_PREV, SA_START_DIAGONAL, SA_START_SECANT, SA_START_GIVEN = range(5)
+SA_START_RANDOM, SA_START_PREV, SA_START_DIAGONAL, SA_START_SECANT, SA_START_GIVEN, SA_START_TANGENT = range(6)
+NCV_MAX = 64          # largest Lanczos basis of the kernels
 
 
 class AlphaParams(C.Structure):
@@ -61,6 +62,48 @@ class LsResult(C.Structure):
 
 
 # name -> (restype, argtypes): every symbol include/specann_b200.h declares
+SA_ADJ_GRADIENT, SA_ADJ_TANGENT, SA_ADJ_SOLVE = range(3)
+
+
+class AdjointParams(C.Structure):
+    _fields_ = [("alpha", C.c_double), ("lambda1", C.c_double), ("beta", C.c_double), ("tol", C.c_double),
+                ("maxiter", C.c_int32), ("mode", C.c_int32), ("y", C.c_void_p), ("rhs", C.c_void_p),
+                ("out", C.c_void_p), ("grad", C.c_void_p)]
+
+
+class AdjointResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("spmv_count", C.c_int32),
+                ("reserved", C.c_int32), ("residual", C.c_double), ("loss", C.c_double),
+                ("dloss_dalpha", C.c_double)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("eigsh_tol", C.c_double), ("pred_tol", C.c_double), ("shift_eps", C.c_double),
+                ("secant_gamma", C.c_double), ("subset_fraction", C.c_double), ("final_sweep_fraction", C.c_double),
+                ("num_alphas", C.c_int32), ("maxiter", C.c_int32), ("ncv", C.c_int32), ("pred_mode", C.c_int32),
+                ("warm_start", C.c_int32), ("residual_check", C.c_int32), ("use_local_search", C.c_int32),
+                ("max_local_iterations", C.c_int32), ("final_sweep_iters", C.c_int32), ("num_rounds", C.c_int32),
+                ("ls_semantics", C.c_int32), ("reserved", C.c_int32)]
+
+
+class BatchAlphaRecord(C.Structure):
+    _fields_ = [("alpha", C.c_double), ("lambda1", C.c_double), ("rho", C.c_double), ("gershgorin", C.c_double),
+                ("residual", C.c_double), ("pred_residual", C.c_double), ("degree_scale", C.c_double),
+                ("signature", C.c_uint64), ("status", C.c_int32), ("iterations", C.c_int32),
+                ("restarts", C.c_int32), ("spmv_count", C.c_int32), ("pred_accepted", C.c_int32),
+                ("retry", C.c_int32), ("converged", C.c_int32), ("candidate", C.c_int32)]
+
+
+class BatchSummary(C.Structure):
+    _fields_ = [("status", C.c_int32), ("num_candidates", C.c_int32), ("ls_iterations", C.c_int32),
+                ("ls_final_passes", C.c_int32), ("alphas_skipped", C.c_int32), ("alphas_retried", C.c_int32),
+                ("team_first_block", C.c_int32), ("team_blocks", C.c_int32), ("integer_gains", C.c_int32),
+                ("reserved", C.c_int32), ("ls_total_flips", C.c_int64), ("device_ms", C.c_double),
+                ("energy_before", C.c_double * 128), ("energy_after", C.c_double * 128)]
+
+
+_I32P = C.POINTER(C.c_int32)
+
 SIGNATURES = {
     "sa_version": (C.c_char_p, []),
     "sa_spmv_scaled_noalloc": (C.c_int, [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
@@ -88,6 +131,22 @@ SIGNATURES = {
     "sa_local_search": (C.c_int, [C.c_void_p, C.POINTER(LsParams), C.c_void_p, C.c_size_t,
                                   C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(LsResult)]),
     "sa_energies": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t, C.POINTER(C.c_double)]),
+    "sa_set_exponent_offsets": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "sa_adjoint_workspace_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
+    "sa_adjoint": (C.c_int, [C.c_void_p, C.POINTER(AdjointParams), C.c_void_p, C.c_size_t,
+                             C.POINTER(AdjointResult)]),
+    "sa_batch_grid": (C.c_int, [C.c_int32, C.c_int32, _I32P]),
+    "sa_batch_plan": (C.c_int, [C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int32, C.c_double,
+                                C.c_double, _I32P, _I32P, _I32P, _I32P]),
+    "sa_batch_workspace_size": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_int32,
+                                          C.c_int32, _I32P, _I32P, _I32P, C.POINTER(C.c_size_t)]),
+    "sa_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p), C.c_int32,
+                                  C.POINTER(C.c_uint64), C.c_int32, C.c_int32, C.c_int32, _I32P, _I32P, _I32P,
+                                  C.c_void_p, C.c_size_t, C.c_void_p]),
+    "sa_batch_sweep": (C.c_int, [C.c_void_p, C.POINTER(BatchConfig), C.POINTER(C.c_double), C.c_int32]),
+    "sa_batch_results": (C.c_int, [C.c_void_p, C.POINTER(BatchAlphaRecord), C.POINTER(BatchSummary)]),
+    "sa_batch_candidate": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
+    "sa_batch_destroy": (C.c_int, [C.c_void_p]),
 }
 
 GRAPH_SIGNATURES = {

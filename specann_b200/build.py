@@ -19,7 +19,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 CUDA_LIB = "libspecann_b200.so"
 GRAPH_LIB = "libspecann_graphs.so"
-CU_SOURCES = ["capi.cu", "alpha.cu", "ls.cu", "noalloc.cu"]
+CU_SOURCES = ["capi.cu", "alpha.cu", "ls.cu", "batch.cu", "adjoint.cu", "noalloc.cu"]
 HEADERS = ["common.cuh", "handle.cuh", "spmv.cuh", "policy.cuh", "alpha_body.cuh", "ls_body.cuh"]
 
 
@@ -37,19 +37,35 @@ def _stale(target: Path, sources) -> bool:
     return any(Path(s).stat().st_mtime > t for s in sources)
 
 
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+              "--extended-lambda", "-Xcompiler", "-fPIC"]
+
+
 def build_cuda(verbose: bool = False, force: bool = False) -> Path:
+    """Compile every .cu to an object in parallel (build/ under the package), then link."""
+    from concurrent.futures import ThreadPoolExecutor
     out = PKG / CUDA_LIB
     srcs = [CSRC / s for s in CU_SOURCES]
-    deps = srcs + [CSRC / h for h in HEADERS] + [ROOT / "include" / "specann_b200.h"]
-    if not force and not _stale(out, deps):
+    common = [CSRC / h for h in HEADERS] + [ROOT / "include" / "specann_b200.h"]
+    if not force and not _stale(out, srcs + common):
         return out
-    cmd = [nvcc_path(), "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-           "--extended-lambda", "-Xcompiler", "-fPIC", "-shared", "-o", str(out),
-           f"-I{ROOT / 'include'}"]
-    if verbose:
-        cmd += ["-Xptxas", "-v"]
-    cmd += [str(s) for s in srcs]
-    subprocess.run(cmd, check=True)
+    objdir = PKG / "build"
+    objdir.mkdir(exist_ok=True)
+    nvcc = nvcc_path()
+
+    def compile_one(src: Path) -> Path:
+        obj = objdir / (src.stem + ".o")
+        if force or _stale(obj, [src] + common):
+            cmd = [nvcc] + NVCC_FLAGS + [f"-I{ROOT / 'include'}", "-c", "-o", str(obj), str(src)]
+            if verbose:
+                cmd += ["-Xptxas", "-v"]
+            subprocess.run(cmd, check=True)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(srcs)) as ex:
+        objs = list(ex.map(compile_one, srcs))
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(out)]
+                   + [str(o) for o in objs], check=True)
     return out
 
 

@@ -25,6 +25,7 @@ static int launch_alpha(sa_handle* h, const sa_alpha_params* p) {
   A.ldv = h->ldv;
   A.sigma = (T*)h->sigma;
   A.ld = h->ld;
+  A.aoff = h->aoff;
   A.V = (T*)h->V;
   A.w = (T*)h->w;
   A.u = (T*)h->u;

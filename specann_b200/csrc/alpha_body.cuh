@@ -36,6 +36,7 @@ struct AlphaArgs {
   long long n, ldv;
   T* sigma;
   const double* ld;
+  const double* aoff;    // per-vertex exponent offsets (a_i = alpha + aoff[i]) or null
   T* V;
   T* w;
   T* u;
@@ -61,7 +62,7 @@ struct AlphaArgs {
 
 // Number of eigenvalues of the tridiagonal (a, b; size m) below x: sign changes of the leading
 // principal minors det(T_k - x I), computed with the three-term recurrence and rescaling.
-__device__ int sturm_count(const double* a, const double* b, int m, double x) {
+__device__ inline int sturm_count(const double* a, const double* b, int m, double x) {
   double pp = 1.0, pc = a[0] - x;
   bool neg = pc < 0.0;
   int cnt = neg ? 1 : 0;
@@ -80,7 +81,7 @@ __device__ int sturm_count(const double* a, const double* b, int m, double x) {
 }
 
 // s_last^2 of the unit eigenvector for eigenvalue x: -det(T_{m-1} - x) / det'(T_m - x).
-__device__ double last_component_sq(const double* a, const double* b, int m, double x) {
+__device__ inline double last_component_sq(const double* a, const double* b, int m, double x) {
   double pp = 1.0, pc = a[0] - x, dp = 0.0, dc = -1.0;
   for (int i = 1; i < m; ++i) {
     const double bb = b[i - 1] * b[i - 1];
@@ -100,7 +101,7 @@ __device__ double last_component_sq(const double* a, const double* b, int m, dou
 }
 
 // Smallest eigenvalue by multisection over the whole CTA (blockDim.x points per round).
-__device__ double smallest_eig_block(const double* a, const double* b, int m) {
+__device__ inline double smallest_eig_block(const double* a, const double* b, int m) {
   __shared__ double s_lo, s_hi;
   __shared__ int s_first;
   if (threadIdx.x == 0) {
@@ -140,7 +141,7 @@ __device__ double smallest_eig_block(const double* a, const double* b, int m) {
 
 // Unit eigenvector of the tridiagonal for eigenvalue theta by inverse iteration (one thread):
 // LU with partial pivoting of (T - theta I), two solves from a constant start.
-__device__ void tridiag_eigvec(const double* a, const double* b, int m, double theta, double* s) {
+__device__ inline void tridiag_eigvec(const double* a, const double* b, int m, double theta, double* s) {
   if (m == 1) { s[0] = 1.0; return; }
   double dl[kNcvMax], d[kNcvMax], du[kNcvMax], du2[kNcvMax];
   int ipiv[kNcvMax];
@@ -200,7 +201,7 @@ __device__ void tridiag_eigvec(const double* a, const double* b, int m, double t
 }
 
 // The (q+1)-th smallest eigenvalue of the tridiagonal by bisection on the Sturm count.
-__device__ double kth_eig(const double* a, const double* b, int m, int q) {
+__device__ inline double kth_eig(const double* a, const double* b, int m, int q) {
   double lo = 1e300, hi = -1e300;
   for (int i = 0; i < m; ++i) {
     const double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i + 1 < m ? fabs(b[i]) : 0.0);
@@ -222,7 +223,7 @@ __device__ double kth_eig(const double* a, const double* b, int m, int q) {
 // Td with the rotations accumulated in Qd (both m x m, row-major). Afterwards Qd^T T Qd has a
 // leading kk x kk tridiagonal, written back to a and b, and the residual of the kept basis is
 // V Q[:, kk] T+[kk][kk-1] + w Q[m-1][kk-1] (w: the pending unnormalised Lanczos vector).
-__device__ void implicit_restart(AlphaCtrl* C, double* Td, double* Qd, int m, int kk) {
+__device__ inline void implicit_restart(AlphaCtrl* C, double* Td, double* Qd, int m, int kk) {
   __shared__ double s_ritz[kNcvMax];
   __shared__ double s_c, s_s;
   const int t = threadIdx.x;
@@ -322,7 +323,7 @@ __device__ __forceinline__ void st16(T* p, const T* in) {
 // ---- reductions of per-CTA partials --------------------------------------------------------
 
 // Sum part[blk * pw + col] over blocks for cols [0, ncols) into out[col] (fixed order).
-__device__ void reduce_partials(const double* part, int pw, int nblocks, int ncols, double* out) {
+__device__ inline void reduce_partials(const double* part, int pw, int nblocks, int ncols, double* out) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int c = wid; c < ncols; c += nw) {
     double acc = 0.0;
@@ -378,12 +379,13 @@ __device__ __forceinline__ unsigned long long word_mix(long long widx, unsigned 
 
 // ---- the alpha-solve kernel ----------------------------------------------------------------
 
-template <typename T, typename RP, class Pol>
+// NW: warps per CTA at most (sizes the shared staging).
+template <typename T, typename RP, class Pol, int NW = kWarps>
 __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol& pol) {
-  __shared__ double sm[kWarps * (kDotBatch + 1)];
+  __shared__ double sm[NW * (kDotBatch + 1)];
   __shared__ double sh[kNcvMax];
   __shared__ double s_theta, s_s2;
-  __shared__ SpmvSmem<T> ssp;
+  __shared__ SpmvSmem<T, NW> ssp;
   __shared__ double sq[kNcvMax * (kDotBatch + 1)];
   AlphaCtrl* C = A.ctrl;
   const long long n = A.n;
@@ -409,7 +411,7 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
   int mode = P.start_mode;
   if (pol.block() == 0 && threadIdx.x == 0) {
     C->mode = mode;
-    C->test_pred = (mode == SA_START_DIAGONAL || mode == SA_START_SECANT) ? 1 : 0;
+    C->test_pred = (mode == SA_START_DIAGONAL || mode == SA_START_SECANT || mode == SA_START_TANGENT) ? 1 : 0;
     C->pred_accepted = -1;
     C->pred_residual = nan("");
     C->iters = 0;
@@ -426,7 +428,8 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
     double ds = 0.0;
     for (long long i = gtid; i < n; i += nthreads) {
       const double ldi = (double)A.ld[i];
-      const double logD = (P.alpha == 0.0) ? 0.0 : P.alpha * ldi;
+      const double ai = A.aoff ? P.alpha + A.aoff[i] : P.alpha;
+      const double logD = (ai == 0.0) ? 0.0 : ai * ldi;
       const double logDc = fmax(logD, kLog2Clamp);
       A.sigma[i] = (T)exp2(-0.5 * logDc - A.half_log2_c);
       ds += exp2(logD);
@@ -470,6 +473,9 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
         x = (double)A.ylast[i];
       } else if (mode == SA_START_GIVEN) {
         x = (double)A.v0[i];
+      } else if (mode == SA_START_TANGENT) {
+        // first-order step along the eigenvector tangent dy/dalpha at alpha_prev (given in v0)
+        x = (double)(T)(A.ylast[i] + (T)(P.alpha - P.alpha_prev) * A.v0[i]);
       } else if (mode == SA_START_DIAGONAL) {
         const double ldi = fmax((double)A.ld[i], kLog2Clamp);
         const T wgt = (T)exp2(0.5 * (P.alpha - P.alpha_prev) * ldi);
@@ -493,7 +499,7 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
           if (threadIdx.x == 0) {
             const int md = C->mode;
             const double nrm = sqrt(sh[0]);
-            const double nin = (md == SA_START_RANDOM) ? 0.0 : (md == SA_START_SECANT ? 2.0 : 1.0);
+            const double nin = (md == SA_START_RANDOM) ? 0.0 : ((md == SA_START_SECANT || md == SA_START_TANGENT) ? 2.0 : 1.0);
             C->bytes += (double)n * sizeof(T) * (2.0 + nin) + (md == SA_START_DIAGONAL ? 8.0 * n : 0.0);
             C->action = ACT_NEXT;
             if (md == SA_START_DIAGONAL && nrm < kTinyNorm) {
@@ -502,6 +508,9 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
             } else if (md == SA_START_SECANT &&
                        (!A.has_prev || sqrt(sh[1]) < kTinyNorm || nrm < kTinyNorm)) {
               C->mode = SA_START_PREV;             // utils/predictors.py:44-55
+              C->action = ACT_P0_AGAIN;
+            } else if (md == SA_START_TANGENT && (!A.has_last || !(nrm >= kTinyNorm) || !isfinite(nrm))) {
+              C->mode = SA_START_PREV;             // as the secant fallback
               C->action = ACT_P0_AGAIN;
             } else if (!(nrm > 0.0) || !isfinite(nrm)) {
               C->status = SA_ERR_NONFINITE;

@@ -406,6 +406,7 @@ int sa_set_matrix(sa_handle* h, const void* rowptr, const int32_t* col, const vo
     return SA_ERR_OOM;
   h->n_items = (long long)items.size();
   h->n_mc = (long long)mc_base.size();
+  h->n_long_part = n_part;
   if (!items.empty())
     SA_CUDA(cudaMemcpyAsync(h->items, items.data(), sizeof(WorkItem) * items.size(), cudaMemcpyHostToDevice, h->stream));
   if (!mc_base.empty()) {
@@ -468,9 +469,10 @@ int sa_alpha_solve(sa_handle* h, const sa_alpha_params* p, sa_alpha_record* rec)
   if (p->ncv < 2 || p->ncv > h->ncv_max || p->ncv > std::max<long long>(2, h->n) || p->maxiter < 1)
     return SA_ERR_INVALID_ARG;
   const int m = p->start_mode;
-  if (m < SA_START_RANDOM || m > SA_START_GIVEN) return SA_ERR_INVALID_ARG;
-  if ((m == SA_START_PREV || m == SA_START_DIAGONAL || m == SA_START_SECANT) && !h->has_last) return SA_ERR_INVALID_ARG;
-  if (m == SA_START_GIVEN && !p->v0) return SA_ERR_INVALID_ARG;
+  if (m < SA_START_RANDOM || m > SA_START_TANGENT) return SA_ERR_INVALID_ARG;
+  if ((m == SA_START_PREV || m == SA_START_DIAGONAL || m == SA_START_SECANT || m == SA_START_TANGENT) && !h->has_last)
+    return SA_ERR_INVALID_ARG;
+  if ((m == SA_START_GIVEN || m == SA_START_TANGENT) && !p->v0) return SA_ERR_INVALID_ARG;
   SA_CUDA(cudaMemsetAsync(h->actrl, 0, sizeof(GridSync), h->stream));
   if (h->n_mc) SA_CUDA(cudaMemsetAsync(h->mc_count, 0, 4 * h->n_mc, h->stream));
   int st = alpha_solve_impl(h, p);

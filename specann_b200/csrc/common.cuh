@@ -47,12 +47,13 @@ __device__ __forceinline__ int ld_volatile_i32(const int* p) {
   return *((volatile const int*)p);
 }
 
-// Grid-wide barrier for a cooperative launch, with an epilogue run by the last CTA to arrive
-// (the whole CTA runs it, after every other CTA's writes are visible) before the others are
-// released. Waits are bounded: after kSpinLimit sleeps the barrier records
-// SA_ERR_BARRIER_TIMEOUT in gs->error and returns false; the caller must then return.
+// Barrier of `expected` co-resident CTAs (a cooperative grid, or a team of CTAs inside one),
+// with an epilogue run by the last CTA to arrive (the whole CTA runs it, after every other CTA's
+// writes are visible) before the others are released. Waits are bounded: after kSpinLimit sleeps
+// the barrier records SA_ERR_BARRIER_TIMEOUT in gs->error and returns false; the caller must then
+// return.
 template <class Epilogue>
-__device__ __forceinline__ bool grid_barrier(GridSync* gs, Epilogue&& epi) {
+__device__ __forceinline__ bool grid_barrier_n(GridSync* gs, unsigned int expected, Epilogue&& epi) {
   __shared__ unsigned int s_last, s_gen;
   __shared__ int s_err;
   __syncthreads();
@@ -60,7 +61,7 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, Epilogue&& epi) {
     s_gen = ld_volatile_u32(&gs->gen);
     __threadfence();
     unsigned int arrived = atomicAdd(&gs->count, 1u);
-    s_last = (arrived == gridDim.x - 1) ? 1u : 0u;
+    s_last = (arrived == expected - 1) ? 1u : 0u;
     s_err = 0;
   }
   __syncthreads();
@@ -90,8 +91,13 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, Epilogue&& epi) {
   return s_err == 0;
 }
 
+template <class Epilogue>
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, Epilogue&& epi) {
+  return grid_barrier_n(gs, gridDim.x, epi);
+}
+
 __device__ __forceinline__ bool grid_barrier(GridSync* gs) {
-  return grid_barrier(gs, [] {});
+  return grid_barrier_n(gs, gridDim.x, [] {});
 }
 
 // ---------------------------------------------------------------------------------------------

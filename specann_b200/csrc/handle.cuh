@@ -65,7 +65,7 @@ struct LsCtrl {
 
 struct Layout {
   size_t total = 0;
-  size_t off(size_t bytes) {
+  __host__ __device__ size_t off(size_t bytes) {
     size_t o = total;
     total += (bytes + 255) & ~size_t(255);
     return o;
@@ -101,6 +101,7 @@ struct sa_handle {
   long long ldv = 0;            // leading dimension of basis vectors (n rounded up to 64)
   void* sigma = nullptr;        // D^{-1/2} / sqrt(c) for the current alpha (T)
   double* ld = nullptr;         // log2 d (double)
+  const double* aoff = nullptr; // per-vertex exponent offsets of the solves (caller's device array) or null
   double* deg = nullptr;        // absolute degrees (double)
   void* V = nullptr;            // Lanczos basis, ncv_max x ldv (T)
   void* w = nullptr;
@@ -115,6 +116,7 @@ struct sa_handle {
   long long n_mc = 0, cap_mc = 0;
   void* long_part = nullptr;
   long long cap_long_part = 0;
+  long long n_long_part = 0;    // partial sums the bound matrix's multi-chunk rows use
   double* blk_part = nullptr;
   int blk_part_width = 0;
   sa::AlphaCtrl* actrl = nullptr;

@@ -40,11 +40,12 @@ struct SpmvArgs {
   T* long_part;
 };
 
-// Per-warp shared staging of a tile: kSegMax products and kSegRows + 1 row offsets.
-template <typename T>
+// Per-warp shared staging of a tile: kSegMax products and kSegRows + 1 row offsets, for CTAs of
+// at most NW warps.
+template <typename T, int NW = kWarps>
 struct SpmvSmem {
-  T prod[kWarps][kSegMax];
-  int rp[kWarps][kSegRows + 1];
+  T prod[NW][kSegMax];
+  int rp[NW][kSegRows + 1];
 };
 
 template <bool kReadOnlyU, typename T>
@@ -86,9 +87,9 @@ __device__ __forceinline__ void load_tile(const int* col, const T* val, const Ti
 }
 
 // fin(row, sum) is called exactly once per row with sum = sum_j val_ij * u_j (T arithmetic).
-template <typename T, typename RP, bool kReadOnlyU = false, class Fin>
+template <typename T, typename RP, bool kReadOnlyU = false, int NW = kWarps, class Fin>
 __device__ __forceinline__ void spmv_items(const SpmvArgs<T, RP>& S, const T* u, long long gwarp,
-                                           long long nwarps, SpmvSmem<T>& sm, Fin&& fin) {
+                                           long long nwarps, SpmvSmem<T, NW>& sm, Fin&& fin) {
   const int lane = threadIdx.x & 31;
   const int wid = threadIdx.x >> 5;
   T* prod = sm.prod[wid];

@@ -14,7 +14,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import AlphaParams, AlphaRecord, LsParams, LsResult, check
+from ._lib import AdjointParams, AdjointResult, AlphaParams, AlphaRecord, LsParams, LsResult, check
 
 
 def _require_cuda():
@@ -218,6 +218,34 @@ class Engine:
         e = (C.c_double * k)()
         check("sa_energies", self.lib.sa_energies(self.h, int(k), C.c_void_p(ptr), nbytes, e))
         return np.array(e[:])
+
+    # ---- differentiation form ----------------------------------------------------------------
+    def set_exponent_offsets(self, offsets: Optional[torch.Tensor]):
+        """Per-vertex exponent offsets (a_i = alpha + offsets_i) of the following solves and
+        adjoints; None clears them. The tensor (float64, on the device) is kept alive here."""
+        self._offsets = None if offsets is None else offsets.to(self.device, torch.float64).contiguous()
+        ptr = C.c_void_p(self._offsets.data_ptr()) if self._offsets is not None else None
+        check("sa_set_exponent_offsets", self.lib.sa_set_exponent_offsets(self.h, ptr))
+
+    def adjoint(self, mode: int, *, alpha: float, lambda1: float, y: torch.Tensor, beta: float = 8.0,
+                tol: float = 1e-6, maxiter: int = 2000, rhs: Optional[torch.Tensor] = None,
+                out: Optional[torch.Tensor] = None, grad: Optional[torch.Tensor] = None) -> AdjointResult:
+        nbytes = C.c_size_t(0)
+        check("sa_adjoint_workspace_size", self.lib.sa_adjoint_workspace_size(self.h, C.byref(nbytes)))
+        need = int(nbytes.value) + 256
+        if getattr(self, "adj_workspace", None) is None or self.adj_workspace.numel() < need:
+            self.adj_workspace = torch.empty(need, dtype=torch.uint8, device=self.device)
+        ptr = (self.adj_workspace.data_ptr() + 255) & ~255
+        p = AdjointParams(alpha=float(alpha), lambda1=float(lambda1), beta=float(beta), tol=float(tol),
+                          maxiter=int(maxiter), mode=int(mode), y=C.c_void_p(y.data_ptr()),
+                          rhs=C.c_void_p(rhs.data_ptr()) if rhs is not None else None,
+                          out=C.c_void_p(out.data_ptr()) if out is not None else None,
+                          grad=C.c_void_p(grad.data_ptr()) if grad is not None else None)
+        res = AdjointResult()
+        check("sa_adjoint", self.lib.sa_adjoint(self.h, C.byref(p), C.c_void_p(ptr), int(nbytes.value), C.byref(res)))
+        if res.status not in (_lib.SA_OK, _lib.SA_ERR_NOT_CONVERGED):
+            check("sa_adjoint", res.status)
+        return res
 
 
 class _CudaArray:

@@ -62,3 +62,25 @@ def drop_isolated(J: sp.csr_matrix) -> sp.csr_matrix:
     if keep.size == J.shape[0]:
         return J
     return J[keep][:, keep].tocsr()
+
+
+def ragged_batch(count: int = 64, seed: int = 2025, log2_min: int = 10, log2_max: int = 17):
+    """The batched ragged workload: `count` instances with n log-uniform in [2^log2_min, 2^log2_max]
+    (seeded); even-numbered ones Erdos-Renyi with expected degree 20, odd-numbered ones
+    Barabasi-Albert with m = 10 or 20; +-1 couplings from a fair coin per undirected edge; isolated
+    nodes removed. Returns a list of (name, CSR)."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(2.0 ** log2_min), np.log(2.0 ** log2_max), count)).astype(np.int64)
+    ms = np.where(rng.random(count) < 0.5, 10, 20)
+    out = []
+    for i in range(count):
+        n = int(sizes[i])
+        gseed = int(rng.integers(1, 2 ** 62))
+        if i % 2 == 0:
+            J = erdos_renyi(n, 20.0 / (n - 1), seed=gseed, couplings="pm1")
+            name = f"er_{n}_{i}"
+        else:
+            J = barabasi_albert(n, int(ms[i]), seed=gseed, couplings="pm1")
+            name = f"ba_{n}_m{int(ms[i])}_{i}"
+        out.append((name, drop_isolated(J)))
+    return out

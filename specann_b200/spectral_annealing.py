@@ -20,12 +20,15 @@ from typing import List, Optional
 
 import numpy as np
 import scipy.sparse as sp
+import torch
 
 from . import _lib
 from .failures import EigensolverBreakdown, NumericalFailure, is_numerical, is_out_of_memory
 from . import results as _results
 
-PRED_MODES = ("diagonal", "secant", "prev")
+# "tangent" (first-order step along dy/dalpha from the eigenvector adjoint) has no reference
+# counterpart; the other three are utils/predictors.py and models/spectral_annealing.py:589-612
+PRED_MODES = ("diagonal", "secant", "prev", "tangent")
 LS_POLICIES = ("default", "fixed_guard", "adaptive_guard", "independent_set", "sequential_oracle")
 SCHEDULES = ("sqrt", "linear")
 
@@ -156,6 +159,8 @@ class SpectralAnnealing:
         # write_results=False skips the result CSVs (the reference writes them after its timer)
         self.write_results = bool(kwargs.pop("write_results", True))
         self.profile = bool(kwargs.pop("profile", False))
+        # MINRES tolerance of the tangent predictor's direction (pred_mode "tangent")
+        self.tangent_tol = float(kwargs.pop("tangent_tol", 1e-4))
         # local-search pass semantics: "priority" (independent flips, monotone) or "snapshot"
         self.ls_semantics = str(kwargs.pop("ls_semantics", "priority"))
         if self.ls_semantics not in ("priority", "snapshot"):
@@ -176,10 +181,11 @@ class SpectralAnnealing:
 
     # -- one alpha ---------------------------------------------------------------------------------
     def _attempt(self, eng, alpha, alpha_prev, rho, g, start_mode, stream_id, ncv):
+        v0 = self._tangent if start_mode == _lib.SA_START_TANGENT else None
         rec = eng.alpha_solve(alpha=alpha, alpha_prev=alpha if alpha_prev is None else alpha_prev, rho=rho,
                               gershgorin=g, tol=self.eigsh_tol, pred_tol=self.pred_tol,
                               maxiter=self.eigsh_maxiter, ncv=ncv, start_mode=start_mode, seed=self._seed,
-                              stream_id=stream_id, align=True, residual_check=self.residual_check)
+                              stream_id=stream_id, align=True, residual_check=self.residual_check, v0=v0)
         if rec.status in (_lib.SA_ERR_BREAKDOWN, _lib.SA_ERR_NONFINITE) or rec.nonfinite:
             raise EigensolverBreakdown(f"Lanczos failed: {_lib.STATUS_NAMES.get(rec.status, rec.status)}")
         if rec.status not in (_lib.SA_OK, _lib.SA_ERR_NOT_CONVERGED):
@@ -201,6 +207,8 @@ class SpectralAnnealing:
             mode = _lib.SA_START_PREV
         elif self.pred_mode == "diagonal":
             mode = _lib.SA_START_DIAGONAL
+        elif self.pred_mode == "tangent":
+            mode = _lib.SA_START_TANGENT if self._tangent is not None else _lib.SA_START_PREV
         else:
             mode = _lib.SA_START_SECANT
         retry = False
@@ -274,6 +282,7 @@ class SpectralAnnealing:
         self._alphas_retried = 0
         self._alpha_errors = 0
         self._last_alpha_error = None
+        self._tangent = None
         for alpha_idx, alpha in enumerate(alpha_list):
             t_alpha = time.time()
             try:
@@ -293,6 +302,15 @@ class SpectralAnnealing:
             lambda1 = rho - rec.mu
             bound = (-0.5 * lambda1 * rec.degree_scale * info.c) if converged else float("nan")
             slot = cands.add_scratch(rec.signature)
+            tangent_spmvs = 0
+            if self.pred_mode == "tangent" and not self.disable_warm_start:
+                # dy/dalpha at this eigenpair (the next alpha's start is y + dalpha t)
+                y_now = eng.result_vector()
+                t = torch.empty_like(y_now)
+                tres = eng.adjoint(_lib.SA_ADJ_TANGENT, alpha=alpha, lambda1=lambda1, y=y_now,
+                                   tol=self.tangent_tol, maxiter=self.eigsh_maxiter, out=t)
+                self._tangent = t
+                tangent_spmvs = int(tres.spmv_count)
             if not self.disable_warm_start:
                 eng.commit()
                 warm = True
@@ -312,6 +330,7 @@ class SpectralAnnealing:
                 'candidate': slot if self.use_local_search else None,
                 'eigsh_residual': rec.residual, 'eigsh_restarts': int(rec.restarts),
                 'eigsh_spmvs': int(rec.spmv_count), 'alg_bytes': float(rec.alg_bytes),
+                'tangent_spmvs': tangent_spmvs,
                 'timestamp': datetime.now().strftime('%Y-%m-%d %H:%M:%S')})
             row_cand.append(slot)
         sweep_end = time.time()
@@ -350,7 +369,6 @@ class SpectralAnnealing:
             best_energy = float(-0.5 * s64 @ (Jc @ s64))
         self._sweep_time = sweep_end - start_time
         self._post_sweep_time = total_time - self._sweep_time
-        import torch
         self._gpu_pool_bytes = int(torch.cuda.memory_reserved())
         if best_alpha is None:
             if self.write_results:

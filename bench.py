@@ -56,6 +56,16 @@ def parse():
     return ap.parse_args()
 
 
+def traffic_ratio():
+    """DRAM bytes / algorithmic bytes of one captured alpha_kernel launch (ncu, committed under
+    profiles/), or None when no capture has been summarised."""
+    p = ROOT / "profiles" / "alpha_kernel_traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    return float(d["dram_bytes"]) / float(d["alg_bytes"])
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -546,7 +556,13 @@ def main():
                    "best_energy": float(energies[-1]) if energies else None},
         "e2e": {"value": e2e_s / world, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": alpha_gbs, "peak": hbm, "unit": "GB/s",
-                     "frac": (alpha_gbs / hbm) if alpha_gbs else None, "traffic": None,
+                     "frac": (alpha_gbs / hbm) if alpha_gbs else None,
+                     "traffic": (traffic_ratio() * st["alpha_bytes"] / max(1, st["alpha_launches"]))
+                     if traffic_ratio() else None,
+                     "traffic_note": "bytes per alpha_kernel launch: the DRAM/algorithmic ratio of one ncu "
+                                     "capture (profiles/alpha_kernel_traffic.json) times this run's mean "
+                                     "algorithmic bytes per launch",
+                     "alg_bytes_per_launch": st["alpha_bytes"] / max(1, st["alpha_launches"]),
                      "kernel": "alpha_kernel (persistent: fused SpMV + Lanczos + rounding)",
                      "peak_source": peak_kind,
                      "alpha_kernel_ms_per_solve": st["alpha_ms"], "alpha_launches_per_solve": st["alpha_launches"],

@@ -270,6 +270,8 @@ typedef struct {
   int32_t integer_gains, reserved;
   int64_t ls_total_flips;
   double device_ms;
+  double phase_ms[6];            /* sweep time by phase as sa_alpha_record.phase_ms, summed over alphas */
+  double ls_ms;                  /* local-search time */
   double energy_before[128];     /* per candidate slot, exact integers for integer couplings */
   double energy_after[128];
 } sa_batch_summary;
@@ -277,14 +279,15 @@ typedef struct {
 /* CTAs of the batch kernel that fit on this device at once (the grid of every batch launch). */
 int sa_batch_grid(int32_t precision, int32_t rowptr64, int32_t* blocks);
 
-/* Host-only plan of problems onto teams of CTAs: the problems (sizes n, nnz) sorted by a cost
- * model, each large one given its own team of about split x its share of `blocks` CTAs, the rest
- * placed longest-first on the team that finishes first (barrier_cost: relative overhead of a
- * multi-CTA team). Outputs team_of[n_prob] and the contiguous teams [team_b0, team_b0 + team_nb)
- * (arrays of `blocks` entries; *n_teams used). No counterpart in the reference. */
-int sa_batch_plan(int32_t n_prob, const int64_t* n, const int64_t* nnz, int32_t blocks, double split,
-                  double barrier_cost, int32_t* team_of, int32_t* team_b0, int32_t* team_nb,
-                  int32_t* n_teams);
+/* Host-only plan of problems onto teams of CTAs: the problems sorted by cost (measured_cost[p],
+ * the CTA-time of an earlier run, or NULL for a model of sizes n, nnz), each large one given its
+ * own team of about split x its share of `blocks` CTAs, the rest placed longest-first on the team
+ * that finishes first (barrier_cost: relative overhead of a multi-CTA team). Outputs
+ * team_of[n_prob] and the contiguous teams [team_b0, team_b0 + team_nb) (arrays of `blocks`
+ * entries; *n_teams used). No counterpart in the reference. */
+int sa_batch_plan(int32_t n_prob, const int64_t* n, const int64_t* nnz, const double* measured_cost,
+                  int32_t blocks, double split, double barrier_cost, int32_t* team_of, int32_t* team_b0,
+                  int32_t* team_nb, int32_t* n_teams);
 
 int sa_batch_workspace_size(int32_t n_inst, sa_handle* const* inst, int32_t seeds_per_instance,
                             int32_t ncv_max, int32_t capacity, int32_t n_teams, const int32_t* team_b0,

@@ -99,6 +99,7 @@ class BatchSummary(C.Structure):
                 ("ls_final_passes", C.c_int32), ("alphas_skipped", C.c_int32), ("alphas_retried", C.c_int32),
                 ("team_first_block", C.c_int32), ("team_blocks", C.c_int32), ("integer_gains", C.c_int32),
                 ("reserved", C.c_int32), ("ls_total_flips", C.c_int64), ("device_ms", C.c_double),
+                ("phase_ms", C.c_double * 6), ("ls_ms", C.c_double),
                 ("energy_before", C.c_double * 128), ("energy_after", C.c_double * 128)]
 
 
@@ -136,8 +137,8 @@ SIGNATURES = {
     "sa_adjoint": (C.c_int, [C.c_void_p, C.POINTER(AdjointParams), C.c_void_p, C.c_size_t,
                              C.POINTER(AdjointResult)]),
     "sa_batch_grid": (C.c_int, [C.c_int32, C.c_int32, _I32P]),
-    "sa_batch_plan": (C.c_int, [C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int32, C.c_double,
-                                C.c_double, _I32P, _I32P, _I32P, _I32P]),
+    "sa_batch_plan": (C.c_int, [C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_double),
+                                C.c_int32, C.c_double, C.c_double, _I32P, _I32P, _I32P, _I32P]),
     "sa_batch_workspace_size": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_int32,
                                           C.c_int32, _I32P, _I32P, _I32P, C.POINTER(C.c_size_t)]),
     "sa_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p), C.c_int32,

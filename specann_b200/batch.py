@@ -40,20 +40,23 @@ def unpack_words(words: np.ndarray, n: int) -> np.ndarray:
     return np.where(bits.reshape(-1)[:n] == 1, 1, -1).astype(np.int8)
 
 
-def plan(n: Sequence[int], nnz: Sequence[int], blocks: int, split: float = 1.0, barrier_cost: float = 0.05):
-    """Host-side plan of problems onto contiguous teams of CTAs (no GPU needed).
-    Returns (team_of[P], team_b0[T], team_nb[T])."""
+def plan(n: Sequence[int], nnz: Sequence[int], blocks: int, split: float = 1.0, barrier_cost: float = 0.05,
+         cost: Optional[Sequence[float]] = None):
+    """Host-side plan of problems onto contiguous teams of CTAs (no GPU needed); `cost`: measured
+    CTA-time per problem (else the size model). Returns (team_of[P], team_b0[T], team_nb[T])."""
     lib = _lib.load()
     P = len(n)
     na = np.ascontiguousarray(n, dtype=np.int64)
     za = np.ascontiguousarray(nnz, dtype=np.int64)
+    ca = None if cost is None else np.ascontiguousarray(cost, dtype=np.float64)
     team_of = np.zeros(P, dtype=np.int32)
     b0 = np.zeros(max(1, blocks), dtype=np.int32)
     nb = np.zeros(max(1, blocks), dtype=np.int32)
     nt = C.c_int32(0)
     I64 = C.POINTER(C.c_int64)
     I32 = C.POINTER(C.c_int32)
-    check("sa_batch_plan", lib.sa_batch_plan(P, na.ctypes.data_as(I64), za.ctypes.data_as(I64), int(blocks),
+    cptr = None if ca is None else ca.ctypes.data_as(C.POINTER(C.c_double))
+    check("sa_batch_plan", lib.sa_batch_plan(P, na.ctypes.data_as(I64), za.ctypes.data_as(I64), cptr, int(blocks),
                                              float(split), float(barrier_cost), team_of.ctypes.data_as(I32),
                                              b0.ctypes.data_as(I32), nb.ctypes.data_as(I32), C.byref(nt)))
     return team_of, b0[:nt.value].copy(), nb[:nt.value].copy()
@@ -105,6 +108,7 @@ class BatchedSpectralAnnealing:
         self.lib = _lib.load()
         self._batch = None
         self._ws = None
+        self._costs = None          # measured CTA-time per problem (autotune), else the size model
         self.engines: List[Engine] = []
         self.Js: List[sp.csr_matrix] = []
         self.last_ms = None
@@ -153,7 +157,7 @@ class BatchedSpectralAnnealing:
             self._batch = None
         blocks = self.grid()
         n, z = self._sizes()
-        team_of, b0, nb = plan(n, z, blocks, split, self.barrier_cost)
+        team_of, b0, nb = plan(n, z, blocks, split, self.barrier_cost, cost=self._costs)
         self.team_of, self.team_b0, self.team_nb = team_of, b0, nb
         I32 = C.POINTER(C.c_int32)
         handles = (C.c_void_p * len(self.engines))(*[e.h.value for e in self.engines])
@@ -213,11 +217,27 @@ class BatchedSpectralAnnealing:
     def _choose_split(self) -> float:
         if self.split is not None:
             return float(self.split)
-        return _TUNED.get(self._key(), 1.0)
+        tuned = _TUNED.get(self._key())
+        if tuned is not None:
+            self._costs = tuned[1]
+            return tuned[0]
+        return 1.0
 
-    def autotune(self, splits=(0.5, 1.0, 2.0, 4.0), num_alphas: int = 8, repeats: int = 1) -> Dict[float, float]:
-        """Time each plan on a short schedule (the first sweep of a plan also warms it up) and keep
-        the fastest for this workload shape. Returns {split: ms}."""
+    def summaries(self) -> List[BatchSummary]:
+        """Per-problem summaries of the last launch (no candidate copies)."""
+        sums = (BatchSummary * self.n_problems)()
+        check("sa_batch_results", self.lib.sa_batch_results(self._batch, None, sums))
+        return list(sums)
+
+    def autotune(self, splits=(1.0, 2.0, 4.0), num_alphas: int = 8, repeats: int = 1) -> Dict[float, float]:
+        """Measure, then choose. A short schedule runs once with the size-model plan; each problem's
+        device time x its team's CTAs becomes its measured cost. Plans built from those costs with
+        each split are then timed on the same short schedule, and the fastest is kept for this
+        workload shape. Returns {split: ms}."""
+        self._costs = None
+        self._build(1.0)
+        self.sweep(num_alphas, use_graph=False)
+        self._costs = [max(1e-3, z.device_ms) * max(1, z.team_blocks) for z in self.summaries()]
         times = {}
         seen = {}
         for s in splits:
@@ -231,7 +251,7 @@ class BatchedSpectralAnnealing:
             times[float(s)] = t
             seen[sig] = float(s)
         best = min(times, key=times.get)
-        _TUNED[self._key()] = best
+        _TUNED[self._key()] = (best, list(self._costs))
         self._build(best)
         self.tuned = times
         return times
@@ -266,6 +286,7 @@ class BatchedSpectralAnnealing:
                    "ls_iterations": int(z.ls_iterations), "ls_final_passes": int(z.ls_final_passes),
                    "alphas_skipped": int(z.alphas_skipped), "alphas_retried": int(z.alphas_retried),
                    "team": (int(z.team_first_block), int(z.team_blocks)), "device_ms": float(z.device_ms),
+                   "phase_ms": [float(x) for x in z.phase_ms], "ls_ms": float(z.ls_ms),
                    "rows": rows, "energy_before": np.array(z.energy_before[:k]),
                    "energy_after": np.array(z.energy_after[:k])}
             best, src = float("inf"), None

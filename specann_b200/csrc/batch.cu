@@ -35,6 +35,7 @@ size_t ls_workspace_bytes(long long n, long long nnz, int k, int integer);
 constexpr int kBatchThreads = 256;
 constexpr int kBatchWarps = kBatchThreads / 32;
 constexpr int kBatchPartWidth = 2 * kNcvMax + kDotBatch + 8;
+constexpr double kPlanStepFloor = 4.0e5;   // latency floor of a Lanczos step, in bytes-equivalent
 
 // One instance (matrix + prelude of its handle), shared by its seeds.
 struct BInstance {
@@ -245,6 +246,7 @@ __device__ bool batch_problem(const BatchArgs& B, const BTeam& tm, int p, const 
     S->ncand = 0; S->skipped = 0; S->retried = 0;
     S->status = SA_OK;
     S->t0 = global_ns();
+    for (int q = 0; q < 6; ++q) pr.sum->phase_ms[q] = 0.0;
   }
   for (long long i = pol.tid(); i < (long long)(I.nnz / (kChunk + 1) + 1); i += pol.nthr()) tm.mc_count[i] = 0;
   if (!pol.sync(nullptr)) return false;
@@ -316,6 +318,8 @@ __device__ bool batch_problem(const BatchArgs& B, const BTeam& tm, int p, const 
       __syncthreads();
       alpha_body<T, RP, TeamPolicy, kBatchWarps>(A, pol);
       if (ld_volatile_i32(&pol.gs->error)) return false;
+      if (pol.block() == 0 && threadIdx.x == 0)
+        for (int q = 0; q < 6; ++q) pr.sum->phase_ms[q] += (double)tm.actrl->tph[q] * 1e-6;
       // decision (models/spectral_annealing.py:614-651): accept, retry cold, or skip the alpha
       if (!pol.sync(nullptr, [&] {
             if (threadIdx.x == 0) {
@@ -431,11 +435,16 @@ __device__ bool batch_problem(const BatchArgs& B, const BTeam& tm, int p, const 
     Z->integer_gains = I.integer_J;
     Z->status = k > 0 ? SA_OK : SA_ERR_BREAKDOWN;
   }
+  const unsigned long long t_ls = global_ns();
   if (k > 0) {
     const bool ok = I.integer_J ? batch_ls<T, RP, int>(B, tm, pr, I, k, pol) : batch_ls<T, RP, double>(B, tm, pr, I, k, pol);
     if (!ok) return false;
   }
-  if (pol.block() == 0 && threadIdx.x == 0) pr.sum->device_ms = (double)(global_ns() - S->t0) * 1e-6;
+  if (pol.block() == 0 && threadIdx.x == 0) {
+    const unsigned long long t1 = global_ns();
+    pr.sum->device_ms = (double)(t1 - S->t0) * 1e-6;
+    pr.sum->ls_ms = (double)(t1 - t_ls) * 1e-6;
+  }
   return true;
 }
 
@@ -600,17 +609,25 @@ int sa_batch_grid(int32_t precision, int32_t rowptr64, int32_t* blocks) {
   return *blocks > 0 ? SA_OK : SA_ERR_CUDA;
 }
 
-int sa_batch_plan(int32_t n_prob, const int64_t* n, const int64_t* nnz, int32_t blocks, double split,
-                  double barrier_cost, int32_t* team_of, int32_t* team_b0, int32_t* team_nb, int32_t* n_teams) {
+int sa_batch_plan(int32_t n_prob, const int64_t* n, const int64_t* nnz, const double* measured_cost, int32_t blocks,
+                  double split, double barrier_cost, int32_t* team_of, int32_t* team_b0, int32_t* team_nb,
+                  int32_t* n_teams) {
   if (n_prob < 1 || !n || !nnz || blocks < 1 || !(split > 0.0) || !(barrier_cost >= 0.0) || !team_of || !team_b0 ||
       !team_nb || !n_teams)
     return SA_ERR_INVALID_ARG;
-  // cost of one Lanczos step in bytes moved: the SpMV stream plus ~24 basis-vector passes
+  // cost of a problem on one CTA: measured (CTA-time of an earlier run), else the model of one
+  // Lanczos step in bytes moved (SpMV stream, ~24 basis-vector passes) plus a latency floor that
+  // dominates for small problems (a step of a few tiles per warp still pays its phases' latency)
   std::vector<double> cost(n_prob);
   double total = 0.0;
   for (int p = 0; p < n_prob; ++p) {
     if (n[p] < 1 || nnz[p] < 0) return SA_ERR_INVALID_ARG;
-    cost[p] = 8.0 * (double)nnz[p] + 100.0 * (double)n[p];
+    if (measured_cost) {
+      if (!(measured_cost[p] > 0.0) || !std::isfinite(measured_cost[p])) return SA_ERR_INVALID_ARG;
+      cost[p] = measured_cost[p];
+    } else {
+      cost[p] = 8.0 * (double)nnz[p] + 100.0 * (double)n[p] + kPlanStepFloor;
+    }
     total += cost[p];
   }
   std::vector<int> ord(n_prob);

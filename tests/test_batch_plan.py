@@ -53,6 +53,16 @@ def test_plan_splits_large_problems_and_balances():
     assert load.max() <= 2.0 * ideal, (load.max(), ideal)
 
 
+def test_plan_with_measured_costs():
+    n, z = c3_sizes(count=16, seeds=1)
+    cost = np.linspace(1.0, 100.0, len(n))[::-1]          # measured CTA-times, largest first
+    team_of, b0, nb = batch.plan(n, z, 32, 1.0, 0.05, cost=cost)
+    assert nb[team_of[0]] >= 2                             # the costliest problem is split
+    assert set(team_of.tolist()) == set(range(len(b0)))
+    with pytest.raises(Exception):
+        batch.plan(n, z, 32, 1.0, 0.05, cost=np.zeros(len(n)))
+
+
 def test_plan_rejects_bad_input():
     with pytest.raises(Exception):
         batch.plan([10, 20], [5, 5], 0)

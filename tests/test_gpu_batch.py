@@ -125,6 +125,7 @@ def test_autotune_picks_a_measured_plan():
     b.load(Js)
     times = b.autotune(splits=(0.5, 4.0), num_alphas=4)
     assert set(times) == {0.5, 4.0} and all(t > 0 for t in times.values())
+    assert b._costs is not None and len(b._costs) == 4
     out = b.solve()
     assert len(out) == 4 and all(np.isfinite(e) for e, _, _ in out)
     b.close()

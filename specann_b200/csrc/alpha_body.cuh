@@ -379,10 +379,15 @@ __device__ __forceinline__ unsigned long long word_mix(long long widx, unsigned 
 
 // ---- the alpha-solve kernel ----------------------------------------------------------------
 
+// Shared scratch of the reductions: per-warp partials of block_store_partials (NW x 9) and the
+// reduced columns of the dot phase (up to 2 kNcvMax + kDotBatch + 8 partial columns).
+constexpr int kRedCols = 2 * kNcvMax + kDotBatch + 8;
+
 // NW: warps per CTA at most (sizes the shared staging).
 template <typename T, typename RP, class Pol, int NW = kWarps>
 __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol& pol) {
-  __shared__ double sm[NW * (kDotBatch + 1)];
+  static_assert(NW * (kDotBatch + 1) <= kRedCols, "reduction scratch too small");
+  __shared__ double sm[kRedCols];
   __shared__ double sh[kNcvMax];
   __shared__ double s_theta, s_s2;
   __shared__ SpmvSmem<T, NW> ssp;

@@ -633,43 +633,50 @@ int sa_batch_plan(int32_t n_prob, const int64_t* n, const int64_t* nnz, const do
   std::vector<int> ord(n_prob);
   std::iota(ord.begin(), ord.end(), 0);
   std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-  const double target = total / (double)blocks;
-  // large problems get teams of several CTAs, sized by split x their share of the grid
+  // Finish time M of the plan: a problem with cost above M gets its own team of
+  // max(2, ceil(split c (1 + barrier_cost) / M)) CTAs; the others share single-CTA teams, as many
+  // as their total cost needs at M. The smallest M whose plan fits in `blocks` CTAs is found by
+  // bisection (the CTA count needed falls as M grows).
+  const double b1 = 1.0 + barrier_cost;
+  auto ctas_for = [&](double M, int* n_small_ctas) {
+    long long need = 0;
+    double small = 0.0;
+    for (int p = 0; p < n_prob; ++p) {
+      if (cost[p] > M) need += std::max(2ll, (long long)std::ceil(split * cost[p] * b1 / M));
+      else small += cost[p];
+    }
+    const int ns = small > 0.0 ? (int)std::max(1.0, std::ceil(small / M)) : 0;
+    if (n_small_ctas) *n_small_ctas = ns;
+    return need + ns;
+  };
+  double lo = total / (double)blocks * 0.5, hi = total * b1 * 2.0 + 1.0;
+  for (int it = 0; it < 200 && hi - lo > 1e-9 * hi; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (ctas_for(mid, nullptr) <= blocks) hi = mid;
+    else lo = mid;
+  }
+  const double M = hi;
+  int n_small_ctas = 0;
+  ctas_for(M, &n_small_ctas);
   struct Team { int nb; double load; };
   std::vector<Team> teams;
-  std::vector<int> team_first_prob;
-  int used = 0;
-  for (int p : ord) {
-    const double want = split * cost[p] / target;
-    int nb = (int)std::lround(want);
-    if (nb < 2) break;                                   // sorted: the rest are single-CTA problems
-    const int left = blocks - used;
-    const bool others = n_prob - (int)teams.size() - 1 > 0;
-    nb = std::min(nb, others ? left - 1 : left);          // keep a CTA for the other problems
-    if (nb < 2) break;
-    teams.push_back({nb, 0.0});
-    team_first_prob.push_back(p);
-    used += nb;
-  }
-  const int n_big = (int)teams.size();
-  for (int b = used; b < blocks; ++b) teams.push_back({1, 0.0});
   for (int p = 0; p < n_prob; ++p) team_of[p] = -1;
-  // time of a problem on a team of nb CTAs: its bytes over nb, plus the barrier overhead of a team
-  auto t_on = [&](int p, int nb) { return cost[p] / (double)nb * (1.0 + (nb > 1 ? barrier_cost : 0.0)); };
-  for (int t = 0; t < n_big; ++t) {
-    team_of[team_first_prob[t]] = t;
-    teams[t].load = t_on(team_first_prob[t], teams[t].nb);
+  auto t_on = [&](int p, int nb) { return cost[p] / (double)nb * (nb > 1 ? b1 : 1.0); };
+  for (int p : ord) {                                    // own teams for the large problems
+    if (cost[p] <= M) continue;
+    const int nb = (int)std::max(2ll, (long long)std::ceil(split * cost[p] * b1 / M));
+    team_of[p] = (int)teams.size();
+    teams.push_back({nb, t_on(p, nb)});
   }
-  for (int p : ord) {                                    // LPT: earliest finishing team
+  const int first_small = (int)teams.size();
+  for (int q = 0; q < n_small_ctas; ++q) teams.push_back({1, 0.0});
+  for (int p : ord) {                                    // LPT over the single-CTA teams
     if (team_of[p] >= 0) continue;
-    int best = -1;
-    double best_t = 0.0;
-    for (int t = 0; t < (int)teams.size(); ++t) {
-      const double ft = teams[t].load + t_on(p, teams[t].nb);
-      if (best < 0 || ft < best_t) { best = t; best_t = ft; }
-    }
+    int best = first_small;
+    for (int t = first_small; t < (int)teams.size(); ++t)
+      if (teams[t].load < teams[best].load) best = t;
     team_of[p] = best;
-    teams[best].load = best_t;
+    teams[best].load += cost[p];
   }
   // drop empty teams, renumber contiguously
   std::vector<int> remap(teams.size(), -1);

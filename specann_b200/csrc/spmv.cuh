@@ -48,6 +48,30 @@ struct SpmvSmem {
   int rp[NW][kSegRows + 1];
 };
 
+// Streaming loads of data read once per SpMV (columns, values, descriptors): read-only path
+// without L1 allocation, so the per-SM L1 keeps the gathered vector (its hub rows are hit again
+// and again) instead of lines that are never reused.
+__device__ __forceinline__ int ld_stream(const int* p) {
+  int v;
+  asm volatile("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ long long ld_stream(const long long* p) {
+  long long v;
+  asm volatile("ld.global.nc.L1::no_allocate.s64 %0, [%1];" : "=l"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float ld_stream(const float* p) {
+  float v;
+  asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ld_stream(const double* p) {
+  double v;
+  asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+
 template <bool kReadOnlyU, typename T>
 __device__ __forceinline__ T gather(const T* u, int j) {
   if (kReadOnlyU) return __ldg(u + j);
@@ -63,9 +87,9 @@ struct TileDesc {
 __device__ __forceinline__ TileDesc load_desc(const WorkItem* items, long long t, long long n_items) {
   TileDesc d{0, 0, 0};
   if (t < n_items) {
-    d.e0 = __ldg(&items[t].e0);
-    d.row = __ldg(&items[t].row);
-    d.meta = __ldg(&items[t].meta);
+    d.e0 = ld_stream(&items[t].e0);
+    d.row = ld_stream(&items[t].row);
+    d.meta = ld_stream(&items[t].meta);
   }
   return d;
 }
@@ -80,8 +104,8 @@ __device__ __forceinline__ void load_tile(const int* col, const T* val, const Ti
     ci[q] = 0;
     v[q] = T(0);
     if (k < len) {
-      ci[q] = __ldg(col + d.e0 + k);
-      v[q] = __ldg(val + d.e0 + k);
+      ci[q] = ld_stream(col + d.e0 + k);
+      v[q] = ld_stream(val + d.e0 + k);
     }
   }
 }

@@ -44,11 +44,16 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-alphas", type=int, default=2)
+    ap.add_argument("--ref-candidates", type=int, default=128,
+                    help="reference arm: distinct candidates of a full solve (the GPU run's count)")
+    ap.add_argument("--ref-ls-passes", type=int, default=1625,
+                    help="reference arm: local-search passes of a full solve (the GPU run's count)")
     ap.add_argument("--spmv-reps", type=int, default=20)
     ap.add_argument("--workload", default="metric", choices=["metric", "batch", "precision", "grad"],
                     help="metric: the headline solve (default); batch: the ragged batched workload "
                          "(64 instances x 4 seeds x 128 alphas, one launch); precision: FP32 + FP64 Ritz vs "
                          "all-FP64 on BA(2^16); grad: the differentiation workload on BA(2^18)")
+    ap.add_argument("--scale-precisions", default="32,64", help="--scale-run: precisions to run, in order")
     ap.add_argument("--scale-run", action="store_true",
                     help="one timed FP32 solve and one timed plain-FP64 solve of the graph, with the energy gap")
     ap.add_argument("--spmv-only", action="store_true",
@@ -137,7 +142,13 @@ def spmv_bytes(n, nnz, rp_bytes, t):
 
 
 def run_reference(args, rank, world):
-    """CPU reference pipeline (oracle port) on a bounded sample, extrapolated to one full solve."""
+    """CPU reference pipeline (the oracle port: SciPy ARPACK eigsh + NumPy local search; the
+    reference's own path is CuPy-only and cannot run on a host) on a bounded sample per step,
+    extrapolated to one full solve: `cpu_sample_alphas` consecutive warm-started alphas (the start
+    rotates with the step) x num_alphas / sample, plus 4 local-search passes over their candidates
+    scaled to `ref_candidates` candidates x `ref_ls_passes` passes (the candidates and passes a full
+    solve of this workload runs; the GPU local search is bit-exact with this one, so its counts
+    apply)."""
     if rank != 0:
         return
     import scipy.sparse as sp
@@ -146,18 +157,24 @@ def run_reference(args, rank, world):
     J = sp.csr_matrix((val.astype(np.float64), col, rowptr.astype(np.int32 if rowptr[-1] < 2**31 else np.int64)),
                       shape=(n, n))
     k = args.cpu_sample_alphas
-    scale = args.num_alphas / k
-    sample = f"{k} consecutive warm-started alphas of {args.num_alphas} + local search of their candidates, x{scale:g}"
     times = []
     for step in range(args.warmup + args.steps):
         start_idx = (step * k) % args.num_alphas
         t0 = time.perf_counter()
-        O.solve(J, precision=args.precision, num_alphas=args.num_alphas, seed=42 + step,
-                alpha_subset=list(range(start_idx, start_idx + k)))
-        dt = (time.perf_counter() - t0) * scale
+        out = O.solve(J, precision=args.precision, num_alphas=args.num_alphas, seed=42 + step,
+                      alpha_subset=list(range(start_idx, min(args.num_alphas, start_idx + k))), use_local_search=False)
+        t_eig = time.perf_counter() - t0
+        S = np.stack(out.candidates) if out.candidates else np.ones((1, n), dtype=np.int8)
+        t0 = time.perf_counter()
+        O.local_search(J, S, seed=42 + step, max_iterations=4, num_rounds=0)
+        t_ls = time.perf_counter() - t0
+        dt = t_eig * args.num_alphas / k + t_ls / 4 / S.shape[0] * args.ref_ls_passes * args.ref_candidates
         if step >= args.warmup:
             times.append(dt)
     value = float(np.mean(times))
+    sample = (f"{k} consecutive warm-started alphas of {args.num_alphas} per step (x{args.num_alphas / k:g}) + 4 "
+              f"local-search passes over their candidates, scaled to {args.ref_candidates} candidates x "
+              f"{args.ref_ls_passes} passes; SciPy ARPACK eigsh and NumPy (single-threaded)")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value * 1000.0, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == 32 else "f64",
@@ -169,19 +186,31 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
-def cpu_baseline_sample(args, n, rowptr, col, val):
+def cpu_baseline_sample(args, n, rowptr, col, val, k_gpu, passes_gpu, ls_sample_passes=4):
+    """The oracle pipeline (SciPy ARPACK eigsh + NumPy local search, one core) on a bounded sample,
+    extrapolated to one full solve: the first `cpu_sample_alphas` warm-started alphas (x num_alphas /
+    sample), plus `ls_sample_passes` local-search passes over their candidates, scaled to the
+    candidates and passes the GPU solve of the same workload used (k_gpu, passes_gpu)."""
     import scipy.sparse as sp
     from oracle import specann_oracle as O
     J = sp.csr_matrix((val.astype(np.float64), col, rowptr.astype(np.int32 if rowptr[-1] < 2**31 else np.int64)),
                       shape=(n, n))
     k = args.cpu_sample_alphas
     t0 = time.perf_counter()
-    O.solve(J, precision=args.precision, num_alphas=args.num_alphas, seed=42, alpha_subset=list(range(k)))
-    dt = time.perf_counter() - t0
-    scale = args.num_alphas / k
-    return {"value": dt * scale, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{k} warm-started alphas of {args.num_alphas} + local search of their candidates "
-                      f"({dt:.1f} s measured), x{scale:g}; SciPy ARPACK eigsh and NumPy, single-threaded"}
+    out = O.solve(J, precision=args.precision, num_alphas=args.num_alphas, seed=42, alpha_subset=list(range(k)),
+                  use_local_search=False)
+    t_eig = time.perf_counter() - t0
+    S = np.stack(out.candidates) if out.candidates else np.ones((1, n), dtype=np.int8)
+    t0 = time.perf_counter()
+    O.local_search(J, S, seed=42, max_iterations=ls_sample_passes, num_rounds=0)
+    t_ls = time.perf_counter() - t0
+    per_pass_per_cand = t_ls / ls_sample_passes / S.shape[0]
+    value = t_eig * args.num_alphas / k + per_pass_per_cand * passes_gpu * k_gpu
+    return {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{k} warm-started alphas of {args.num_alphas} ({t_eig:.1f} s, x{args.num_alphas / k:g}) + "
+                      f"{ls_sample_passes} local-search passes over {S.shape[0]} candidates ({t_ls:.1f} s), scaled to "
+                      f"the GPU solve's {k_gpu} candidates x {passes_gpu} passes; SciPy ARPACK eigsh and NumPy, "
+                      f"single-threaded"}
 
 
 def run_batch(args, rank, world, local):
@@ -409,7 +438,7 @@ def main():
         Jw = _g.barabasi_albert(4096, 8, seed=1)
         SpectralAnnealing("w.txt", "w", random_seed=1, num_alphas=4, write_results=False).solve(Jw)
         d_val64 = None
-        for prec in (32, 64):
+        for prec in [int(x) for x in args.scale_precisions.split(",")]:
             if prec == 64:
                 del d_val
                 torch.cuda.empty_cache()
@@ -435,8 +464,9 @@ def main():
             del s
             torch.cuda.empty_cache()
             print(json.dumps(out), flush=True)
-        e32, e64 = out["fp32"]["best_energy"], out["fp64"]["best_energy"]
-        out["energy_gap_rel"] = abs(e32 - e64) / abs(e64)
+        if "fp32" in out and "fp64" in out:
+            e32, e64 = out["fp32"]["best_energy"], out["fp64"]["best_energy"]
+            out["energy_gap_rel"] = abs(e32 - e64) / abs(e64)
         print(json.dumps(out))
         return
 
@@ -507,7 +537,7 @@ def main():
                "alpha0": float(iters[0]), "restarts": int(sum(r["eigsh_restarts"] for r in s.alpha_results)),
                "pred_accepted": int(sum(1 for r in s.alpha_results if r["pred_accepted"])),
                "max_residual": float(np.nanmax([r["eigsh_residual"] for r in s.alpha_results])),
-               "candidates": int(s._num_candidates or 0)}
+               "candidates": int(s._num_candidates or 0), "ls_passes": int(getattr(s, "_ls_passes", 0))}
     hbm, peak_kind = peaks()
     alpha_gbs = st["alpha_bytes"] / (st["alpha_ms"] / 1000.0) / 1e9 if st["alpha_ms"] > 0 else None
 
@@ -579,7 +609,8 @@ def main():
         "gpu_launches": int(launches),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(args, n, rowptr, col, val)
+        line["cpu_baseline"] = cpu_baseline_sample(args, n, rowptr, col, val, int(s._num_candidates or 1),
+                                                   int(getattr(s, "_ls_passes", 1)))
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -62,6 +62,8 @@ typedef struct {
   const void* v0;        /* device start vector (SA_START_GIVEN) or tangent (SA_START_TANGENT), else NULL */
   int32_t round;         /* 1: round x = D^{-1/2} y to packed spins and hash them */
   int32_t residual_check;/* 1: true residual ||S y - mu y|| with one more SpMV */
+  int32_t restart_keep;  /* Ritz vectors kept by an implicit restart (0: 8; at most 16 and ncv / 2) */
+  int32_t reserved;
 } sa_alpha_params;
 
 typedef struct {

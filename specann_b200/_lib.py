@@ -36,7 +36,7 @@ class AlphaParams(C.Structure):
                 ("secant_gamma", C.c_double), ("maxiter", C.c_int32), ("ncv", C.c_int32),
                 ("start_mode", C.c_int32), ("align", C.c_int32), ("seed", C.c_uint64),
                 ("stream_id", C.c_int64), ("v0", C.c_void_p), ("round", C.c_int32),
-                ("residual_check", C.c_int32)]
+                ("residual_check", C.c_int32), ("restart_keep", C.c_int32), ("reserved", C.c_int32)]
 
 
 class AlphaRecord(C.Structure):
@@ -155,6 +155,9 @@ GRAPH_SIGNATURES = {
     "sa_graph_ba": (C.c_int, [C.c_int64, C.c_int64, C.c_uint64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sa_graph_er_nnz": (C.c_int64, [C.c_int64, C.c_double, C.c_uint64]),
     "sa_graph_er": (C.c_int, [C.c_int64, C.c_double, C.c_uint64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sa_instance_load": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "sa_instance_fetch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

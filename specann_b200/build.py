@@ -5,7 +5,7 @@
 
 Outputs (next to this file):
   libspecann_b200.so   CUDA kernels + the C-ABI of include/specann_b200.h (sm_100a only)
-  libspecann_graphs.so seeded synthetic graph generators (host C++, OpenMP)
+  libspecann_graphs.so seeded synthetic graph generators and the instance loader (host C++, OpenMP)
 """
 import argparse
 import os
@@ -70,12 +70,13 @@ def build_cuda(verbose: bool = False, force: bool = False) -> Path:
 
 
 def build_graphs(force: bool = False) -> Path:
+    """Host library: seeded graph generators and the native instance loader."""
     out = PKG / GRAPH_LIB
-    src = CSRC / "graphgen.cpp"
-    if not force and not _stale(out, [src]):
+    srcs = [CSRC / "graphgen.cpp", CSRC / "loader.cpp"]
+    if not force and not _stale(out, srcs):
         return out
     cxx = shutil.which("g++") or "g++"
-    subprocess.run([cxx, "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", str(out), str(src)],
+    subprocess.run([cxx, "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", str(out)] + [str(s) for s in srcs],
                    check=True)
     return out
 

@@ -28,6 +28,8 @@ enum Action : int { ACT_NEXT = 0, ACT_REPASS = 1, ACT_RESTART = 2, ACT_REJECT = 
                     ACT_P0_AGAIN = 6 };
 
 constexpr double kLog2Clamp = -39.86313713864835;   // log2(1e-12)
+constexpr int kRestartDefault = 8;   // Ritz vectors kept by an implicit restart (at most ncv / 2)
+constexpr int kRestartMax = 16;
 constexpr double kTinyNorm = 1e-12;
 
 template <typename T, typename RP>
@@ -391,7 +393,7 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
   __shared__ double sh[kNcvMax];
   __shared__ double s_theta, s_s2;
   __shared__ SpmvSmem<T, NW> ssp;
-  __shared__ double sq[kNcvMax * (kDotBatch + 1)];
+  __shared__ double sq[kNcvMax * (kRestartMax + 1)];
   AlphaCtrl* C = A.ctrl;
   const long long n = A.n;
   const long long gtid = pol.tid();
@@ -749,7 +751,8 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
               }
               __syncthreads();
               if (C->action == ACT_RESTART) {
-                const int kk = max(1, min(kDotBatch, ncv / 2));
+                const int keep = P.restart_keep > 0 ? P.restart_keep : kRestartDefault;
+                const int kk = max(1, min(min(keep, kRestartMax), ncv / 2));
                 implicit_restart(C, A.dense, A.dense + kNcvMax * kNcvMax, m, kk);
               }
             }
@@ -775,22 +778,22 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
         __syncthreads();
         double v[1] = {0.0};
         for (long long i = gtid; i < n; i += nthreads) {
-          double y[kDotBatch + 1];
+          double y[kRestartMax + 1];
 #pragma unroll
-          for (int c = 0; c <= kDotBatch; ++c) y[c] = 0.0;
-#pragma unroll 4
+          for (int c = 0; c <= kRestartMax; ++c) y[c] = 0.0;
+#pragma unroll 2
           for (int r = 0; r < m; ++r) {
             const double vr = (double)A.V[(long long)r * A.ldv + i];
 #pragma unroll
-            for (int c = 0; c <= kDotBatch; ++c)
+            for (int c = 0; c <= kRestartMax; ++c)
               if (c <= kk) y[c] += vr * sq[r * (kk + 1) + c];
           }
 #pragma unroll
-          for (int c = 0; c < kDotBatch; ++c)
+          for (int c = 0; c < kRestartMax; ++c)
             if (c < kk) A.V[(long long)c * A.ldv + i] = (T)y[c];
           double yk = 0.0;
 #pragma unroll
-          for (int c = 0; c <= kDotBatch; ++c)
+          for (int c = 0; c <= kRestartMax; ++c)
             if (c == kk) yk = y[c];
           const T f = (T)(yk * beta_hat + (double)A.w[i] * sig_q);
           A.w[i] = f;

@@ -32,7 +32,7 @@ namespace sa {
 
 size_t ls_workspace_bytes(long long n, long long nnz, int k, int integer);
 
-constexpr int kBatchThreads = 256;
+constexpr int kBatchThreads = 128;
 constexpr int kBatchWarps = kBatchThreads / 32;
 constexpr int kBatchPartWidth = 2 * kNcvMax + kDotBatch + 8;
 constexpr double kPlanStepFloor = 4.0e5;   // latency floor of a Lanczos step, in bytes-equivalent
@@ -449,7 +449,7 @@ __device__ bool batch_problem(const BatchArgs& B, const BTeam& tm, int p, const 
 }
 
 template <typename T, typename RP>
-__global__ void __launch_bounds__(kBatchThreads, 2) batch_kernel(BatchArgs B) {
+__global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(BatchArgs B) {
   __shared__ int s_team;
   if (threadIdx.x == 0) {
     s_team = -1;
@@ -633,16 +633,21 @@ int sa_batch_plan(int32_t n_prob, const int64_t* n, const int64_t* nnz, const do
   std::vector<int> ord(n_prob);
   std::iota(ord.begin(), ord.end(), 0);
   std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-  // Finish time M of the plan: a problem with cost above M gets its own team of
-  // max(2, ceil(split c (1 + barrier_cost) / M)) CTAs; the others share single-CTA teams, as many
-  // as their total cost needs at M. The smallest M whose plan fits in `blocks` CTAs is found by
-  // bisection (the CTA count needed falls as M grows).
+  // Finish time M of the plan: a problem whose cost exceeds M gets its own team of
+  // nb = ceil(split c (1 + barrier_cost) / M) CTAs when that is 2 or more; the others share
+  // single-CTA teams, as many as their total cost needs at M. The smallest M whose plan fits in
+  // `blocks` CTAs is found by bisection (the CTA count needed falls as M grows).
   const double b1 = 1.0 + barrier_cost;
+  auto team_size = [&](int p, double M) -> long long {
+    if (cost[p] <= M) return 1;
+    return (long long)std::ceil(split * cost[p] * b1 / M);
+  };
   auto ctas_for = [&](double M, int* n_small_ctas) {
     long long need = 0;
     double small = 0.0;
     for (int p = 0; p < n_prob; ++p) {
-      if (cost[p] > M) need += std::max(2ll, (long long)std::ceil(split * cost[p] * b1 / M));
+      const long long nb = team_size(p, M);
+      if (nb >= 2) need += nb;
       else small += cost[p];
     }
     const int ns = small > 0.0 ? (int)std::max(1.0, std::ceil(small / M)) : 0;
@@ -663,8 +668,8 @@ int sa_batch_plan(int32_t n_prob, const int64_t* n, const int64_t* nnz, const do
   for (int p = 0; p < n_prob; ++p) team_of[p] = -1;
   auto t_on = [&](int p, int nb) { return cost[p] / (double)nb * (nb > 1 ? b1 : 1.0); };
   for (int p : ord) {                                    // own teams for the large problems
-    if (cost[p] <= M) continue;
-    const int nb = (int)std::max(2ll, (long long)std::ceil(split * cost[p] * b1 / M));
+    const int nb = (int)team_size(p, M);
+    if (nb < 2) continue;
     team_of[p] = (int)teams.size();
     teams.push_back({nb, t_on(p, nb)});
   }

@@ -48,34 +48,59 @@ struct SpmvSmem {
   int rp[NW][kSegRows + 1];
 };
 
-// Streaming loads of data read once per SpMV (columns, values, descriptors): read-only path
-// without L1 allocation, so the per-SM L1 keeps the gathered vector (its hub rows are hit again
-// and again) instead of lines that are never reused.
-__device__ __forceinline__ int ld_stream(const int* p) {
+// L2 cache policies (createpolicy): the streams read once per SpMV (columns, values, descriptors)
+// are first in line for eviction and skip L1, so L1 and L2 keep the gathered vector (its hub rows
+// are hit again and again; at large n it is about the size of L2), whose gathers are marked
+// evict_last.
+__device__ __forceinline__ unsigned long long l2_policy_evict_first() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ unsigned long long l2_policy_evict_last() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ int ld_stream(const int* p, unsigned long long pol) {
   int v;
-  asm volatile("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
   return v;
 }
-__device__ __forceinline__ long long ld_stream(const long long* p) {
+__device__ __forceinline__ long long ld_stream(const long long* p, unsigned long long pol) {
   long long v;
-  asm volatile("ld.global.nc.L1::no_allocate.s64 %0, [%1];" : "=l"(v) : "l"(p));
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(pol));
   return v;
 }
-__device__ __forceinline__ float ld_stream(const float* p) {
+__device__ __forceinline__ float ld_stream(const float* p, unsigned long long pol) {
   float v;
-  asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
   return v;
 }
-__device__ __forceinline__ double ld_stream(const double* p) {
+__device__ __forceinline__ double ld_stream(const double* p, unsigned long long pol) {
   double v;
-  asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
+// Gathers of the SpMV's input vector (read-only path when it is immutable for the kernel).
+__device__ __forceinline__ float ld_gather(const float* p, unsigned long long pol, bool nc) {
+  float v;
+  if (nc) asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  else asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_gather(const double* p, unsigned long long pol, bool nc) {
+  double v;
+  if (nc) asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  else asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
   return v;
 }
 
 template <bool kReadOnlyU, typename T>
-__device__ __forceinline__ T gather(const T* u, int j) {
-  if (kReadOnlyU) return __ldg(u + j);
-  return u[j];
+__device__ __forceinline__ T gather(const T* u, int j, unsigned long long pol) {
+  return ld_gather(u + j, pol, kReadOnlyU);
 }
 
 struct TileDesc {
@@ -84,19 +109,20 @@ struct TileDesc {
   int meta;
 };
 
-__device__ __forceinline__ TileDesc load_desc(const WorkItem* items, long long t, long long n_items) {
+__device__ __forceinline__ TileDesc load_desc(const WorkItem* items, long long t, long long n_items,
+                                              unsigned long long pol) {
   TileDesc d{0, 0, 0};
   if (t < n_items) {
-    d.e0 = ld_stream(&items[t].e0);
-    d.row = ld_stream(&items[t].row);
-    d.meta = ld_stream(&items[t].meta);
+    d.e0 = ld_stream(&items[t].e0, pol);
+    d.row = ld_stream(&items[t].row, pol);
+    d.meta = ld_stream(&items[t].meta, pol);
   }
   return d;
 }
 
 template <typename T>
 __device__ __forceinline__ void load_tile(const int* col, const T* val, const TileDesc& d, int lane,
-                                          int (&ci)[kTileIt], T (&v)[kTileIt]) {
+                                          int (&ci)[kTileIt], T (&v)[kTileIt], unsigned long long pol) {
   const int len = item_len(d.meta);
 #pragma unroll
   for (int q = 0; q < kTileIt; ++q) {
@@ -104,8 +130,8 @@ __device__ __forceinline__ void load_tile(const int* col, const T* val, const Ti
     ci[q] = 0;
     v[q] = T(0);
     if (k < len) {
-      ci[q] = ld_stream(col + d.e0 + k);
-      v[q] = ld_stream(val + d.e0 + k);
+      ci[q] = ld_stream(col + d.e0 + k, pol);
+      v[q] = ld_stream(val + d.e0 + k, pol);
     }
   }
 }
@@ -118,24 +144,26 @@ __device__ __forceinline__ void spmv_items(const SpmvArgs<T, RP>& S, const T* u,
   const int wid = threadIdx.x >> 5;
   T* prod = sm.prod[wid];
   int* srp = sm.rp[wid];
+  const unsigned long long pol_stream = l2_policy_evict_first();
+  const unsigned long long pol_gather = l2_policy_evict_last();
   long long it = gwarp;
-  TileDesc cur = load_desc(S.items, it, S.n_items);
+  TileDesc cur = load_desc(S.items, it, S.n_items, pol_stream);
   int ci[kTileIt];
   T v[kTileIt];
-  load_tile(S.col, S.val, cur, lane, ci, v);
-  TileDesc nxt = load_desc(S.items, it + nwarps, S.n_items);
+  load_tile(S.col, S.val, cur, lane, ci, v, pol_stream);
+  TileDesc nxt = load_desc(S.items, it + nwarps, S.n_items, pol_stream);
   while (it < S.n_items) {
     // stage 1: next tile's entries and the descriptor after it are put in flight
     int cn[kTileIt];
     T vn[kTileIt];
-    load_tile(S.col, S.val, nxt, lane, cn, vn);
-    const TileDesc nn = load_desc(S.items, it + 2 * nwarps, S.n_items);
+    load_tile(S.col, S.val, nxt, lane, cn, vn, pol_stream);
+    const TileDesc nn = load_desc(S.items, it + 2 * nwarps, S.n_items, pol_stream);
     // stage 2: the current tile
     const int len = item_len(cur.meta);
 #pragma unroll
     for (int q = 0; q < kTileIt; ++q) {
       const int k = lane + 32 * q;
-      if (k < len) v[q] *= gather<kReadOnlyU>(u, ci[q]);
+      if (k < len) v[q] *= gather<kReadOnlyU>(u, ci[q], pol_gather);
     }
     if (cur.row >= 0) {
       const int nr = item_nrows(cur.meta);

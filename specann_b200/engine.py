@@ -109,13 +109,14 @@ class Engine:
     # ---- one alpha --------------------------------------------------------------------------
     def alpha_solve(self, *, alpha, alpha_prev, rho, gershgorin, tol, pred_tol, maxiter, ncv, start_mode,
                     seed, stream_id, align=True, v0: Optional[torch.Tensor] = None, secant_gamma=1.0,
-                    round_spins=True, residual_check=True) -> AlphaRecord:
+                    round_spins=True, residual_check=True, restart_keep=0) -> AlphaRecord:
         p = AlphaParams(alpha=float(alpha), alpha_prev=float(alpha_prev), rho=float(rho),
                         gershgorin=float(gershgorin), tol=float(tol), pred_tol=float(pred_tol),
                         secant_gamma=float(secant_gamma), maxiter=int(maxiter), ncv=int(ncv),
                         start_mode=int(start_mode), align=int(bool(align)), seed=int(seed) & (2 ** 64 - 1),
                         stream_id=int(stream_id), v0=C.c_void_p(v0.data_ptr()) if v0 is not None else None,
-                        round=int(bool(round_spins)), residual_check=int(bool(residual_check)))
+                        round=int(bool(round_spins)), residual_check=int(bool(residual_check)),
+                        restart_keep=int(restart_keep))
         rec = AlphaRecord()
         if self.profile:
             e0 = torch.cuda.Event(enable_timing=True)

@@ -160,7 +160,9 @@ class SpectralAnnealing:
         self.write_results = bool(kwargs.pop("write_results", True))
         self.profile = bool(kwargs.pop("profile", False))
         # MINRES tolerance of the tangent predictor's direction (pred_mode "tangent")
-        self.tangent_tol = float(kwargs.pop("tangent_tol", 1e-4))
+        self.tangent_tol = float(kwargs.pop("tangent_tol", 1e-2))
+        # Ritz vectors kept by an implicit restart of the Lanczos basis (0: the kernel's default, 8)
+        self.restart_keep = int(kwargs.pop("restart_keep", 0))
         # local-search pass semantics: "priority" (independent flips, monotone) or "snapshot"
         self.ls_semantics = str(kwargs.pop("ls_semantics", "priority"))
         if self.ls_semantics not in ("priority", "snapshot"):
@@ -185,7 +187,8 @@ class SpectralAnnealing:
         rec = eng.alpha_solve(alpha=alpha, alpha_prev=alpha if alpha_prev is None else alpha_prev, rho=rho,
                               gershgorin=g, tol=self.eigsh_tol, pred_tol=self.pred_tol,
                               maxiter=self.eigsh_maxiter, ncv=ncv, start_mode=start_mode, seed=self._seed,
-                              stream_id=stream_id, align=True, residual_check=self.residual_check, v0=v0)
+                              stream_id=stream_id, align=True, residual_check=self.residual_check, v0=v0,
+                              restart_keep=self.restart_keep)
         if rec.status in (_lib.SA_ERR_BREAKDOWN, _lib.SA_ERR_NONFINITE) or rec.nonfinite:
             raise EigensolverBreakdown(f"Lanczos failed: {_lib.STATUS_NAMES.get(rec.status, rec.status)}")
         if rec.status not in (_lib.SA_OK, _lib.SA_ERR_NOT_CONVERGED):
@@ -390,6 +393,7 @@ class SpectralAnnealing:
         if self.ls_batch:
             eb, ea, res = eng.local_search(k, max_iterations=self.max_local_iterations, seed=self._seed,
                                            semantics=self.ls_semantics)
+            self._ls_passes = int(res.iterations) + int(res.final_passes)
             return eb, ea, int(res.iterations)
         eb = np.empty(k)
         ea = np.empty(k)

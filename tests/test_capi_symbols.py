@@ -51,7 +51,7 @@ def test_workspace_size_is_host_only(lib_path):
 
 def test_struct_layouts_match_c():
     # sizes of the C structs on x86-64 (natural alignment)
-    assert ctypes.sizeof(_lib.AlphaParams) == 7 * 8 + 4 * 4 + 8 + 8 + 8 + 2 * 4
+    assert ctypes.sizeof(_lib.AlphaParams) == 7 * 8 + 4 * 4 + 8 + 8 + 8 + 4 * 4
     assert ctypes.sizeof(_lib.AlphaRecord) == 4 * 4 + 7 * 8 + 8 + 4 * 4 + 8 + 6 * 8
     assert ctypes.sizeof(_lib.LsParams) == 4 * 3 + 4 + 2 * 8 + 2 * 4 + 8 + 2 * 4
     assert ctypes.sizeof(_lib.LsResult) == 4 * 4 + 8

@@ -653,26 +653,27 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
         const long long nvec = n / VW;
         for (long long iv = gtid; iv < nvec; iv += nthreads) {
           const long long i0 = iv * VW;
+          // w and sigma are put in flight first; the basis is read kDotBatch vectors at a time
+          T wv[VW], sg[VW], uv[VW];
+          ld16(A.w + i0, wv);
+          ld16(A.sigma + i0, sg);
           double corr[VW];
 #pragma unroll
           for (int r = 0; r < VW; ++r) corr[r] = 0.0;
-          for (int kb = 0; kb <= j; kb += 4) {
-            T vk[4][VW];
+          for (int kb = 0; kb <= j; kb += kDotBatch) {
+            T vk[kDotBatch][VW];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < kDotBatch; ++q) {
               if (kb + q <= j) ld16(A.V + (long long)(kb + q) * A.ldv + i0, vk[q]);
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < kDotBatch; ++q) {
               if (kb + q <= j) {
 #pragma unroll
                 for (int r = 0; r < VW; ++r) corr[r] += sh[kb + q] * (double)vk[q][r];
               }
             }
           }
-          T wv[VW], sg[VW], uv[VW];
-          ld16(A.w + i0, wv);
-          ld16(A.sigma + i0, sg);
 #pragma unroll
           for (int r = 0; r < VW; ++r) {
             wv[r] = (T)((double)wv[r] - corr[r]);

@@ -46,8 +46,9 @@ def parse():
     ap.add_argument("--cpu-sample-alphas", type=int, default=2)
     ap.add_argument("--ref-candidates", type=int, default=128,
                     help="reference arm: distinct candidates of a full solve (the GPU run's count)")
-    ap.add_argument("--ref-ls-passes", type=int, default=1625,
-                    help="reference arm: local-search passes of a full solve (the GPU run's count)")
+    ap.add_argument("--ref-ls-passes", type=int, default=89,
+                    help="reference arm: local-search passes of a full solve (89: the count of the default "
+                         "workload's solve, seed 42, whose local search is bit-exact with the CPU one)")
     ap.add_argument("--spmv-reps", type=int, default=20)
     ap.add_argument("--workload", default="metric", choices=["metric", "batch", "precision", "grad"],
                     help="metric: the headline solve (default); batch: the ragged batched workload "

@@ -102,10 +102,19 @@ __device__ inline double last_component_sq(const double* a, const double* b, int
   return s2;
 }
 
-// Smallest eigenvalue by multisection over the whole CTA (blockDim.x points per round).
-__device__ inline double smallest_eig_block(const double* a, const double* b, int m) {
-  __shared__ double s_lo, s_hi;
+// Smallest eigenvalue by multisection over the whole CTA (blockDim.x points per round), and the
+// squared last component of its unit eigenvector in *s2 (every thread gets both). The tridiagonal
+// is first copied from the control block to shared memory: every Sturm count walks it
+// sequentially, so its loads must be short.
+__device__ inline double smallest_eig_block(const double* ag, const double* bg, int m, double* s2) {
+  __shared__ double s_lo, s_hi, s_s2;
   __shared__ int s_first;
+  __shared__ double a[kNcvMax], b[kNcvMax];
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    a[i] = ag[i];
+    b[i] = (i + 1 < m) ? bg[i] : 0.0;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
     double lo = 1e300, hi = -1e300;
     for (int i = 0; i < m; ++i) {
@@ -137,6 +146,9 @@ __device__ inline double smallest_eig_block(const double* a, const double* b, in
     if (s_hi - s_lo <= 1e-15 * fmax(1.0, fabs(s_hi))) break;
   }
   const double r = 0.5 * (s_lo + s_hi);
+  if (threadIdx.x == 0) s_s2 = last_component_sq(a, b, m, r);
+  __syncthreads();
+  *s2 = s_s2;
   __syncthreads();
   return r;
 }
@@ -724,10 +736,11 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
             const int act0 = C->action;
             if (act0 == ACT_NEXT) {
               const int m = j + 1;
-              const double th = smallest_eig_block(C->a, C->b, m);
+              double s2;
+              const double th = smallest_eig_block(C->a, C->b, m, &s2);
               if (threadIdx.x == 0) {
                 s_theta = th;
-                s_s2 = last_component_sq(C->a, C->b, m, th);
+                s_s2 = s2;
               }
               __syncthreads();
               if (threadIdx.x == 0) {

@@ -367,7 +367,10 @@ class SpectralAnnealing:
             kind, c = best_src
             best_spins = eng.candidate_spins(c, refined=(kind == 'refined')).cpu().numpy().astype(self.dtype)
         total_time = time.time() - start_time
-        if best_spins is not None and Jc is not None:
+        if best_spins is not None and Jc is not None and not (info.integer and abs(best_energy) < 2.0 ** 52):
+            # the reported energy is -1/2 s^T J s in FP64 from the input J (models/spectral_annealing.py:
+            # 484-488); for integer couplings the device energy is already that number exactly (int64
+            # sums of int32 fields), so the host product is only needed for non-integer J
             s64 = best_spins.astype(np.float64)
             best_energy = float(-0.5 * s64 @ (Jc @ s64))
         self._sweep_time = sweep_end - start_time

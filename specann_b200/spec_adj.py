@@ -77,7 +77,7 @@ class _FixedAlpha:
         Jc = as_csr(J)
         n = Jc.shape[0]
         self._seed = _seed_value(self.random_seed)
-        data = Jc.data.astype(np.float32) if self.precision == 32 else Jc.data
+        data = Jc.data.astype(np.float32, copy=False) if self.precision == 32 else Jc.data
         eng = Engine(n, Jc.nnz, precision=self.precision, ncv_max=default_ncv(n, None), max_candidates=1)
         self.engine = eng
         info = eng.upload_csr(Jc.indptr, Jc.indices, data)

@@ -237,7 +237,7 @@ class SpectralAnnealing:
         Jc = as_csr(J)
         n = Jc.shape[0]
         eng = self._make_engine(n, Jc.nnz)
-        data = Jc.data.astype(np.float32) if (self.precision == 32) else Jc.data
+        data = Jc.data.astype(np.float32, copy=False) if (self.precision == 32) else Jc.data
         info = eng.upload_csr(Jc.indptr, Jc.indices, data)
         return self._sweep(eng, info, Jc, start_time)
 

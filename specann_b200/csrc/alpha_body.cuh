@@ -233,61 +233,72 @@ __device__ inline double kth_eig(const double* a, const double* b, int m, int q)
 }
 
 // Implicit restart with exact shifts (the CTA): the m - kk largest Ritz values of the tridiagonal
-// (a, b; size m) are the shifts of implicit QR steps, done as Givens bulge chasing on a dense copy
-// Td with the rotations accumulated in Qd (both m x m, row-major). Afterwards Qd^T T Qd has a
-// leading kk x kk tridiagonal, written back to a and b, and the residual of the kept basis is
+// (a, b; size m) are the shifts of implicit QR steps. Each step is a bulge chase on the tridiagonal
+// itself (diagonal d, off-diagonal e and the one bulge entry, O(m) work by one thread: rotation r
+// acts on rows and columns r, r + 1 as T <- G T G^T with G = [[c, s], [-s, c]]); its m - 1 rotations
+// are then applied to the rows of Q (Qd, m x m row-major, Q <- Q G^T) by all threads, one row each,
+// with the row's moving entry kept in a register. Afterwards Q^T T Q has a leading kk x kk
+// tridiagonal, written back to a and b, and the residual of the kept basis is
 // V Q[:, kk] T+[kk][kk-1] + w Q[m-1][kk-1] (w: the pending unnormalised Lanczos vector).
-__device__ inline void implicit_restart(AlphaCtrl* C, double* Td, double* Qd, int m, int kk) {
-  __shared__ double s_ritz[kNcvMax];
-  __shared__ double s_c, s_s;
+// scratch: 5 kNcvMax doubles of shared memory.
+__device__ inline void implicit_restart(AlphaCtrl* C, double* Qd, int m, int kk, double* scratch) {
+  double* d = scratch;
+  double* e = scratch + kNcvMax;
+  double* ritz = scratch + 2 * kNcvMax;
+  double* rc = scratch + 3 * kNcvMax;
+  double* rs = scratch + 4 * kNcvMax;
   const int t = threadIdx.x;
-  if (t < m) s_ritz[t] = kth_eig(C->a, C->b, m, t);
-  for (int idx = t; idx < m * m; idx += blockDim.x) {
-    const int r = idx / m, c = idx % m;
-    double v = 0.0;
-    if (r == c) v = C->a[r];
-    else if (r == c + 1) v = C->b[c];
-    else if (c == r + 1) v = C->b[r];
-    Td[idx] = v;
-    Qd[idx] = (r == c) ? 1.0 : 0.0;
+  for (int i = t; i < m; i += blockDim.x) {
+    d[i] = C->a[i];
+    e[i] = (i + 1 < m) ? C->b[i] : 0.0;
   }
   __syncthreads();
+  if (t < m) ritz[t] = kth_eig(d, e, m, t);
+  for (int idx = t; idx < m * m; idx += blockDim.x) Qd[idx] = (idx / m == idx % m) ? 1.0 : 0.0;
+  __syncthreads();
   for (int sft = m - 1; sft >= kk; --sft) {
-    const double mu = s_ritz[sft];
-    for (int r = 0; r < m - 1; ++r) {
-      if (t == 0) {
-        const double x = (r == 0) ? Td[0] - mu : Td[r * m + (r - 1)];
-        const double z = (r == 0) ? Td[m] : Td[(r + 1) * m + (r - 1)];
+    if (t == 0) {
+      const double mu = ritz[sft];
+      double g = 0.0;                          // bulge T[r+1][r-1]
+      for (int r = 0; r < m - 1; ++r) {
+        const double x = (r == 0) ? d[0] - mu : e[r - 1];
+        const double z = (r == 0) ? e[0] : g;
         const double rr = hypot(x, z);
-        s_c = (rr == 0.0) ? 1.0 : x / rr;
-        s_s = (rr == 0.0) ? 0.0 : z / rr;
+        const double c = (rr == 0.0) ? 1.0 : x / rr;
+        const double sn = (rr == 0.0) ? 0.0 : z / rr;
+        if (r > 0) e[r - 1] = rr;
+        const double dr = d[r], dn = d[r + 1], er = e[r];
+        d[r] = c * c * dr + 2.0 * c * sn * er + sn * sn * dn;
+        d[r + 1] = sn * sn * dr - 2.0 * c * sn * er + c * c * dn;
+        e[r] = c * sn * (dn - dr) + (c * c - sn * sn) * er;
+        if (r + 2 < m) {
+          g = sn * e[r + 1];
+          e[r + 1] = c * e[r + 1];
+        }
+        rc[r] = c;
+        rs[r] = sn;
       }
-      __syncthreads();
-      const double c = s_c, s = s_s;
-      if (t < m) {
-        const double p = Td[r * m + t], q = Td[(r + 1) * m + t];
-        Td[r * m + t] = c * p + s * q;
-        Td[(r + 1) * m + t] = -s * p + c * q;
-      }
-      __syncthreads();
-      if (t < m) {
-        double p = Td[t * m + r], q = Td[t * m + r + 1];
-        Td[t * m + r] = c * p + s * q;
-        Td[t * m + r + 1] = -s * p + c * q;
-        p = Qd[t * m + r];
-        q = Qd[t * m + r + 1];
-        Qd[t * m + r] = c * p + s * q;
-        Qd[t * m + r + 1] = -s * p + c * q;
-      }
-      __syncthreads();
     }
+    __syncthreads();
+    for (int q = t; q < m; q += blockDim.x) {
+      double* row = Qd + (long long)q * m;
+      double pv = row[0];
+      for (int r = 0; r < m - 1; ++r) {
+        const double qv = row[r + 1];
+        const double c = rc[r], sn = rs[r];
+        row[r] = c * pv + sn * qv;
+        pv = -sn * pv + c * qv;
+      }
+      row[m - 1] = pv;
+    }
+    __syncthreads();
   }
   if (t < kk) {
-    C->a[t] = Td[t * m + t];
-    if (t + 1 < kk) C->b[t] = Td[(t + 1) * m + t];
+    C->a[t] = d[t];
+    if (t + 1 < kk) C->b[t] = e[t];
   }
   if (t == 0) {
-    C->irl_beta = Td[kk * m + (kk - 1)];
+    C->irl_beta = e[kk - 1];
     C->irl_sigma = Qd[(m - 1) * m + (kk - 1)];
     C->irl_k = kk;
   }
@@ -767,7 +778,7 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
               if (C->action == ACT_RESTART) {
                 const int keep = P.restart_keep > 0 ? P.restart_keep : kRestartDefault;
                 const int kk = max(1, min(min(keep, kRestartMax), ncv / 2));
-                implicit_restart(C, A.dense, A.dense + kNcvMax * kNcvMax, m, kk);
+                implicit_restart(C, A.dense + kNcvMax * kNcvMax, m, kk, sq);
               }
             }
           })) return;

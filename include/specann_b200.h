@@ -134,6 +134,27 @@ int sa_set_matrix(sa_handle* h, const void* rowptr, const int32_t* col, const vo
  * device vectors of the handle's precision. */
 int sa_spmv_scaled(sa_handle* h, double alpha, double rho, const void* x, void* y);
 
+/* SpMV stream policy (every kernel that applies the operator). packed_columns = 1 (the default):
+ * when every coupling of the bound matrix has the same magnitude w, the SpMV streams one int32 per
+ * entry (the column with the coupling's sign in bit 31) instead of the column and the value; the
+ * products are unchanged. hub_columns = H > 0: gathers of columns below H are kept in L1, the
+ * others bypass it (0, the default: one L1 policy for every gather). Takes effect at the next
+ * launch and survives sa_set_matrix. */
+int sa_set_spmv_policy(sa_handle* h, int32_t packed_columns, int64_t hub_columns);
+/* The policy in effect: packed (1 when the packed stream is used), the common coupling magnitude
+ * (0 when the magnitudes differ) and the hub column count. Any pointer may be NULL. */
+int sa_get_spmv_policy(sa_handle* h, int32_t* packed_columns, double* magnitude, int64_t* hub_columns);
+
+/* Column-panel SpMV. Every CTA keeps the row sums of a block of rows in shared memory and gathers
+ * the scaled input from panels of it staged in shared memory, instead of from L2: it pays when
+ * rows average more than ~20 entries. sa_panel_workspace_size gives the bytes of the layout for
+ * the bound matrix; sa_panel_build lays the matrix out in that caller-owned device workspace
+ * (256-byte aligned, kept until the next sa_set_matrix) and switches the operator kernels to it;
+ * sa_panel_enable(h, 0 / 1) switches back and forth. sa_set_matrix drops the layout. */
+int sa_panel_workspace_size(sa_handle* h, size_t* bytes);
+int sa_panel_build(sa_handle* h, void* workspace, size_t bytes);
+int sa_panel_enable(sa_handle* h, int32_t on);
+
 /* One alpha of the sweep (models/spectral_annealing.py:568-669 with utils/eigsh.py:10-17 and
  * utils/predictors.py): start vector / predictor with its residual test, warm-started
  * thick-restart Lanczos for the smallest eigenpair of S_rho with the Ritz-matrix guard

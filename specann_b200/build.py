@@ -19,8 +19,8 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 CUDA_LIB = "libspecann_b200.so"
 GRAPH_LIB = "libspecann_graphs.so"
-CU_SOURCES = ["capi.cu", "alpha.cu", "ls.cu", "batch.cu", "adjoint.cu", "noalloc.cu"]
-HEADERS = ["common.cuh", "handle.cuh", "spmv.cuh", "policy.cuh", "alpha_body.cuh", "ls_body.cuh"]
+CU_SOURCES = ["capi.cu", "alpha.cu", "ls.cu", "batch.cu", "adjoint.cu", "noalloc.cu", "panel.cu"]
+HEADERS = ["common.cuh", "handle.cuh", "spmv.cuh", "policy.cuh", "alpha_body.cuh", "ls_body.cuh", "panel.cuh"]
 
 
 def nvcc_path() -> str:

@@ -49,6 +49,9 @@ struct BInstance {
   long long n, nnz, W, ldv;
   double c, dmin, dmax, half_log2_c, sqrt_c;
   int integer_J, rp64;
+  const int* scol;   // packed signed columns (one coupling magnitude wmag) or null
+  double wmag;
+  int hub, pad;
 };
 
 // Sweep state of the problem a team is running (written in barrier epilogues).
@@ -271,6 +274,9 @@ __device__ bool batch_problem(const BatchArgs& B, const BTeam& tm, int p, const 
         A.S.mc_base = I.mc_base;
         A.S.mc_count = tm.mc_count;
         A.S.long_part = (T*)tm.long_part;
+        A.S.scol = I.scol;
+        A.S.wmag = (T)I.wmag;
+        A.S.hub = I.hub;
         A.n = n;
         A.ldv = I.ldv;
         A.sigma = (T*)tm.sigma;
@@ -783,6 +789,10 @@ int sa_batch_create(sa_batch** out, int32_t n_inst, sa_handle* const* inst, int3
     I.sqrt_c = std::sqrt(h->c);
     I.integer_J = h->integer_J;
     I.rp64 = h->rp64;
+    I.scol = h->packed ? h->scol : nullptr;
+    I.wmag = h->wmag;
+    I.hub = h->hub;
+    I.pad = 0;
   }
   // teams: working arrays
   char* base = b->ws + sz.header;

@@ -32,11 +32,15 @@ using namespace sa;
     if (e_ != cudaSuccess) return SA_ERR_CUDA;          \
   } while (0)
 
+namespace sa {
+int panel_spmv_launch(sa_handle* h, const void* u, const void* x, const void* sigma, double rho, void* y);
+}
+
 namespace {
 
 struct Carve {
   size_t sigma, ld, deg, V, w, u, y0, y1, y2, items, mc_base, mc_count, long_part, blk_part, actrl, red,
-      cand, refined, scratch, dense, total;
+      cand, refined, scratch, dense, scol, total;
 };
 
 constexpr int kMaxBlocks = 1024;
@@ -68,6 +72,7 @@ Carve carve(long long n, long long nnz, int prec, int ncv_max, int max_cand) {
   c.refined = L.off(4 * (size_t)W * max_cand);
   c.scratch = L.off(4 * (size_t)W);
   c.dense = L.off(8 * 2 * (size_t)kNcvMax * kNcvMax);
+  c.scol = L.off(4 * (size_t)std::max(1ll, nnz));
   c.total = L.total;
   return c;
 }
@@ -113,6 +118,19 @@ __global__ void degree_kernel(const RP* rp, const int* col, const T* val, long l
     atomicMin(&red->dmin_bits, s_min);
     if (s_nonint) atomicOr(&red->nonint, 1);
   }
+}
+
+// Packed signed columns for couplings of one magnitude w: scol[k] = col[k] | sign(val[k]) << 31;
+// *mixed is set when some |val[k]| differs from w (then scol is not used).
+template <typename T>
+__global__ void pack_kernel(const int* col, const T* val, long long nnz, T w, int* scol, int* mixed) {
+  int bad = 0;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += (long long)gridDim.x * blockDim.x) {
+    const T v = __ldg(val + k);
+    if (!(fabs(v) == w)) bad = 1;
+    scol[k] = __ldg(col + k) | ((v < T(0)) ? (int)0x80000000u : 0);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(mixed, 1);
 }
 
 __global__ void logdeg_kernel(const double* deg, long long n, double c, double* ld) {
@@ -257,6 +275,13 @@ void build_items(const std::vector<long long>& rp, long long n, std::vector<Work
 
 }  // namespace
 
+template <typename T, typename RP>
+static void set_policy(SpmvArgs<T, RP>& S, const sa_handle* h) {
+  S.scol = h->packed ? h->scol : nullptr;
+  S.wmag = (T)h->wmag;
+  S.hub = h->hub;
+}
+
 extern "C" {
 
 const char* sa_version(void) { return "specann_b200 0.1 (sm_100a)"; }
@@ -320,6 +345,7 @@ int sa_create(sa_handle** out, int64_t n, int64_t nnz, int32_t rowptr64, int32_t
   h->refined = (uint32_t*)(h->ws + c.refined);
   h->scratch = (uint32_t*)(h->ws + c.scratch);
   h->dense = (double*)(h->ws + c.dense);
+  h->scol = (int32_t*)(h->ws + c.scol);
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { delete h; return SA_ERR_CUDA; }
   if (cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) { delete h; return SA_ERR_CUDA; }
@@ -397,6 +423,34 @@ int sa_set_matrix(sa_handle* h, const void* rowptr, const int32_t* col, const vo
   logdeg_kernel<<<g, 256, 0, h->stream>>>(h->deg, h->n, h->c, h->ld);
   count_launches(1);
   SA_CUDA(cudaGetLastError());
+  // one coupling magnitude: the SpMV streams packed signed columns instead of col and val
+  h->wmag = 0.0;
+  h->packed = 0;
+  if (h->nnz > 0) {
+    int* mixed = (int*)(h->red + 16);
+    double w0 = 0.0;
+    SA_CUDA(cudaMemsetAsync(mixed, 0, sizeof(int), h->stream));
+    const int gp = grid_for(h->nnz, 256, h->sm_count);
+    if (h->prec == 32) {
+      float f0 = 0.0f;
+      SA_CUDA(cudaMemcpyAsync(&f0, val, sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+      SA_CUDA(cudaStreamSynchronize(h->stream));
+      w0 = std::fabs((double)f0);
+      pack_kernel<float><<<gp, 256, 0, h->stream>>>(col, (const float*)val, h->nnz, (float)w0, h->scol, mixed);
+    } else {
+      SA_CUDA(cudaMemcpyAsync(&w0, val, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      SA_CUDA(cudaStreamSynchronize(h->stream));
+      w0 = std::fabs(w0);
+      pack_kernel<double><<<gp, 256, 0, h->stream>>>(col, (const double*)val, h->nnz, w0, h->scol, mixed);
+    }
+    count_launches(1);
+    SA_CUDA(cudaGetLastError());
+    int mx = 1;
+    SA_CUDA(cudaMemcpyAsync(&mx, mixed, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    SA_CUDA(cudaStreamSynchronize(h->stream));
+    if (!mx && w0 > 0.0 && std::isfinite(w0)) h->wmag = w0;
+    h->packed = (h->wmag > 0.0 && h->packed_allowed) ? 1 : 0;
+  }
   std::vector<WorkItem> items;
   std::vector<long long> mc_base;
   long long n_part = 0;
@@ -419,6 +473,7 @@ int sa_set_matrix(sa_handle* h, const void* rowptr, const int32_t* col, const vo
   h->blocks = (int)std::max(1ll, std::min((long long)h->max_blocks, want));
   SA_CUDA(cudaStreamSynchronize(h->stream));
   h->bound = true;
+  h->panel_ready = h->panel_on = 0;
   h->has_last = h->has_prev = false;
   if (norm_c) *norm_c = h->c;
   if (d_min) *d_min = h->dmin;
@@ -427,11 +482,36 @@ int sa_set_matrix(sa_handle* h, const void* rowptr, const int32_t* col, const vo
   return SA_OK;
 }
 
+int sa_set_spmv_policy(sa_handle* h, int32_t packed_columns, int64_t hub_columns) {
+  if (!h || hub_columns < 0 || (packed_columns != 0 && packed_columns != 1)) return SA_ERR_INVALID_ARG;
+  h->packed_allowed = packed_columns;
+  h->packed = (h->bound && h->wmag > 0.0 && packed_columns) ? 1 : 0;
+  h->hub = (int)std::min<int64_t>(hub_columns, h->n);
+  return SA_OK;
+}
+
+int sa_get_spmv_policy(sa_handle* h, int32_t* packed_columns, double* magnitude, int64_t* hub_columns) {
+  if (!h) return SA_ERR_INVALID_ARG;
+  if (packed_columns) *packed_columns = h->packed;
+  if (magnitude) *magnitude = h->wmag;
+  if (hub_columns) *hub_columns = h->hub;
+  return SA_OK;
+}
+
 int sa_spmv_scaled(sa_handle* h, double alpha, double rho, const void* x, void* y) {
   if (!h || !h->bound || !x || !y) return SA_ERR_INVALID_ARG;
   const int g = grid_for(h->n, 256, h->sm_count);
   const double hl = 0.5 * std::log2(h->c);
   const int gs = h->sm_count * 2;
+  if (h->panel_on) {
+    if (h->prec == 32)
+      scale_kernel<float><<<g, 256, 0, h->stream>>>(h->ld, h->n, alpha, hl, (const float*)x, (float*)h->sigma, (float*)h->u);
+    else
+      scale_kernel<double><<<g, 256, 0, h->stream>>>(h->ld, h->n, alpha, hl, (const double*)x, (double*)h->sigma, (double*)h->u);
+    count_launches(1);
+    SA_CUDA(cudaGetLastError());
+    return panel_spmv_launch(h, h->u, x, h->sigma, rho, y);
+  }
   if (h->n_mc) SA_CUDA(cudaMemsetAsync(h->mc_count, 0, 4 * h->n_mc, h->stream));
   if (h->prec == 32) {
     scale_kernel<float><<<g, 256, 0, h->stream>>>(h->ld, h->n, alpha, hl, (const float*)x, (float*)h->sigma, (float*)h->u);
@@ -440,10 +520,12 @@ int sa_spmv_scaled(sa_handle* h, double alpha, double rho, const void* x, void* 
     SpmvArgs<float, long long> S64;
     if (h->rp64) {
       S64 = SpmvArgs<float, long long>{(const long long*)h->rowptr, h->col, (const float*)h->val, h->items, h->n_items, h->mc_base, h->mc_count, (float*)h->long_part};
+      set_policy(S64, h);
       spmv_kernel<float, long long><<<gs, kThreads, 0, h->stream>>>(S64, h->group, (const float*)h->u, (const float*)x, (const float*)h->sigma, (float)rho, (float*)y);
       count_launches(1);
     } else {
       S32 = SpmvArgs<float, int>{(const int*)h->rowptr, h->col, (const float*)h->val, h->items, h->n_items, h->mc_base, h->mc_count, (float*)h->long_part};
+      set_policy(S32, h);
       spmv_kernel<float, int><<<gs, kThreads, 0, h->stream>>>(S32, h->group, (const float*)h->u, (const float*)x, (const float*)h->sigma, (float)rho, (float*)y);
       count_launches(1);
     }
@@ -452,10 +534,12 @@ int sa_spmv_scaled(sa_handle* h, double alpha, double rho, const void* x, void* 
     count_launches(1);
     if (h->rp64) {
       SpmvArgs<double, long long> S{(const long long*)h->rowptr, h->col, (const double*)h->val, h->items, h->n_items, h->mc_base, h->mc_count, (double*)h->long_part};
+      set_policy(S, h);
       spmv_kernel<double, long long><<<gs, kThreads, 0, h->stream>>>(S, h->group, (const double*)h->u, (const double*)x, (const double*)h->sigma, rho, (double*)y);
       count_launches(1);
     } else {
       SpmvArgs<double, int> S{(const int*)h->rowptr, h->col, (const double*)h->val, h->items, h->n_items, h->mc_base, h->mc_count, (double*)h->long_part};
+      set_policy(S, h);
       spmv_kernel<double, int><<<gs, kThreads, 0, h->stream>>>(S, h->group, (const double*)h->u, (const double*)x, (const double*)h->sigma, rho, (double*)y);
       count_launches(1);
     }

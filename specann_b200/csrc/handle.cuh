@@ -97,6 +97,19 @@ struct sa_handle {
   bool bound = false;
   double c = 0.0, dmin = 0.0, dmax = 0.0;
   int integer_J = 0;
+  // SpMV stream of couplings of one magnitude: packed signed columns (workspace, nnz int32)
+  int32_t* scol = nullptr;
+  double wmag = 0.0;        // the common |J_ij| when every coupling has it, else 0
+  int packed = 0;           // scol holds the bound matrix and the SpMV streams it
+  int packed_allowed = 1;   // sa_set_spmv_policy
+  int hub = 0;              // L1-resident gather columns [0, hub) (sa_set_spmv_policy)
+  // column-panel SpMV (sa_panel_build): layout in the caller's panel workspace
+  int panel_ready = 0, panel_on = 0;
+  int panel_blocks = 0, panel_count = 0, panel_width = 0;
+  const unsigned int* panel_ent = nullptr;
+  const void* panel_val = nullptr;
+  const long long* panel_chunk = nullptr;
+  const int* panel_row0 = nullptr;
   // workspace carve-out
   long long ldv = 0;            // leading dimension of basis vectors (n rounded up to 64)
   void* sigma = nullptr;        // D^{-1/2} / sqrt(c) for the current alpha (T)

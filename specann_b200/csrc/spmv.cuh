@@ -38,6 +38,15 @@ struct SpmvArgs {
   const long long* mc_base;
   int* mc_count;
   T* long_part;
+  // Couplings of one magnitude (every |val| == wmag): scol[k] = col[k] with the sign of val[k] in
+  // bit 31, streamed instead of col and val (4 bytes per entry instead of 4 + sizeof(T)); null
+  // when the magnitudes differ. The products are the same: val[k] is exactly +-wmag.
+  const int* scol;
+  T wmag;
+  // Gathers of columns below hub stay in L1 (evict_last), the others bypass it (no_allocate);
+  // 0: every gather with the default L1 policy. (No default member initialisers: the batch kernel
+  // keeps these arguments in shared memory; brace-initialised copies zero the trailing fields.)
+  int hub;
 };
 
 // Per-warp shared staging of a tile: kSegMax products and kSegRows + 1 row offsets, for CTAs of
@@ -103,6 +112,37 @@ __device__ __forceinline__ T gather(const T* u, int j, unsigned long long pol) {
   return ld_gather(u + j, pol, kReadOnlyU);
 }
 
+// Gather with an L1 policy chosen by the column: j < hub kept in L1 (evict_last), j >= hub not
+// allocated in L1. One predicated load of each kind, so the warp's loads stay independent.
+__device__ __forceinline__ float ld_gather_hub(const float* p, int j, int hub, unsigned long long pol, bool nc) {
+  float v;
+  if (nc)
+    asm volatile("{\n .reg .pred hp;\n setp.lt.s32 hp, %2, %3;\n"
+                 " @hp ld.global.nc.L1::evict_last.L2::cache_hint.f32 %0, [%1], %4;\n"
+                 " @!hp ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %4;\n}"
+                 : "=f"(v) : "l"(p), "r"(j), "r"(hub), "l"(pol));
+  else
+    asm volatile("{\n .reg .pred hp;\n setp.lt.s32 hp, %2, %3;\n"
+                 " @hp ld.global.L1::evict_last.L2::cache_hint.f32 %0, [%1], %4;\n"
+                 " @!hp ld.global.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %4;\n}"
+                 : "=f"(v) : "l"(p), "r"(j), "r"(hub), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_gather_hub(const double* p, int j, int hub, unsigned long long pol, bool nc) {
+  double v;
+  if (nc)
+    asm volatile("{\n .reg .pred hp;\n setp.lt.s32 hp, %2, %3;\n"
+                 " @hp ld.global.nc.L1::evict_last.L2::cache_hint.f64 %0, [%1], %4;\n"
+                 " @!hp ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %4;\n}"
+                 : "=d"(v) : "l"(p), "r"(j), "r"(hub), "l"(pol));
+  else
+    asm volatile("{\n .reg .pred hp;\n setp.lt.s32 hp, %2, %3;\n"
+                 " @hp ld.global.L1::evict_last.L2::cache_hint.f64 %0, [%1], %4;\n"
+                 " @!hp ld.global.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %4;\n}"
+                 : "=d"(v) : "l"(p), "r"(j), "r"(hub), "l"(pol));
+  return v;
+}
+
 struct TileDesc {
   long long e0;
   int row;
@@ -120,18 +160,33 @@ __device__ __forceinline__ TileDesc load_desc(const WorkItem* items, long long t
   return d;
 }
 
-template <typename T>
-__device__ __forceinline__ void load_tile(const int* col, const T* val, const TileDesc& d, int lane,
+template <typename T, typename RP>
+__device__ __forceinline__ void load_tile(const SpmvArgs<T, RP>& S, const TileDesc& d, int lane,
                                           int (&ci)[kTileIt], T (&v)[kTileIt], unsigned long long pol) {
   const int len = item_len(d.meta);
+  if (S.scol) {
+#pragma unroll
+    for (int q = 0; q < kTileIt; ++q) {
+      const int k = lane + 32 * q;
+      ci[q] = 0;
+      if (k < len) ci[q] = ld_stream(S.scol + d.e0 + k, pol);
+    }
+#pragma unroll
+    for (int q = 0; q < kTileIt; ++q) {
+      v[q] = (ci[q] < 0) ? -S.wmag : S.wmag;
+      ci[q] &= 0x7fffffff;
+      if (lane + 32 * q >= len) v[q] = T(0);
+    }
+    return;
+  }
 #pragma unroll
   for (int q = 0; q < kTileIt; ++q) {
     const int k = lane + 32 * q;
     ci[q] = 0;
     v[q] = T(0);
     if (k < len) {
-      ci[q] = ld_stream(col + d.e0 + k, pol);
-      v[q] = ld_stream(val + d.e0 + k, pol);
+      ci[q] = ld_stream(S.col + d.e0 + k, pol);
+      v[q] = ld_stream(S.val + d.e0 + k, pol);
     }
   }
 }
@@ -150,20 +205,28 @@ __device__ __forceinline__ void spmv_items(const SpmvArgs<T, RP>& S, const T* u,
   TileDesc cur = load_desc(S.items, it, S.n_items, pol_stream);
   int ci[kTileIt];
   T v[kTileIt];
-  load_tile(S.col, S.val, cur, lane, ci, v, pol_stream);
+  load_tile(S, cur, lane, ci, v, pol_stream);
   TileDesc nxt = load_desc(S.items, it + nwarps, S.n_items, pol_stream);
   while (it < S.n_items) {
     // stage 1: next tile's entries and the descriptor after it are put in flight
     int cn[kTileIt];
     T vn[kTileIt];
-    load_tile(S.col, S.val, nxt, lane, cn, vn, pol_stream);
+    load_tile(S, nxt, lane, cn, vn, pol_stream);
     const TileDesc nn = load_desc(S.items, it + 2 * nwarps, S.n_items, pol_stream);
     // stage 2: the current tile
     const int len = item_len(cur.meta);
+    if (S.hub > 0) {
 #pragma unroll
-    for (int q = 0; q < kTileIt; ++q) {
-      const int k = lane + 32 * q;
-      if (k < len) v[q] *= gather<kReadOnlyU>(u, ci[q], pol_gather);
+      for (int q = 0; q < kTileIt; ++q) {
+        const int k = lane + 32 * q;
+        if (k < len) v[q] *= ld_gather_hub(u + ci[q], ci[q], S.hub, pol_gather, kReadOnlyU);
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < kTileIt; ++q) {
+        const int k = lane + 32 * q;
+        if (k < len) v[q] *= gather<kReadOnlyU>(u, ci[q], pol_gather);
+      }
     }
     if (cur.row >= 0) {
       const int nr = item_nrows(cur.meta);

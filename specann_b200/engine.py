@@ -106,6 +106,30 @@ class Engine:
                                                         C.c_void_p(y.data_ptr())))
         return y
 
+    def set_spmv_policy(self, packed_columns: bool = True, hub_columns: int = 0) -> None:
+        """SpMV stream policy: packed signed columns for one-magnitude couplings, and the number
+        of leading columns whose gathers stay in L1 (0: one policy for all)."""
+        check("sa_set_spmv_policy", self.lib.sa_set_spmv_policy(self.h, 1 if packed_columns else 0,
+                                                                int(hub_columns)))
+
+    def build_panels(self) -> int:
+        """Lay the bound matrix out for the column-panel SpMV (a device workspace owned by this
+        engine until the next bind) and switch the operator kernels to it. Returns its bytes."""
+        nb = C.c_size_t(0)
+        check("sa_panel_workspace_size", self.lib.sa_panel_workspace_size(self.h, C.byref(nb)))
+        self._panel_ws = torch.empty(max(256, nb.value), dtype=torch.uint8, device=self.device)
+        check("sa_panel_build", self.lib.sa_panel_build(self.h, C.c_void_p(self._panel_ws.data_ptr()),
+                                                        C.c_size_t(self._panel_ws.numel())))
+        return nb.value
+
+    def enable_panels(self, on: bool = True) -> None:
+        check("sa_panel_enable", self.lib.sa_panel_enable(self.h, 1 if on else 0))
+
+    def spmv_policy(self) -> dict:
+        packed, mag, hub = C.c_int32(0), C.c_double(0.0), C.c_int64(0)
+        check("sa_get_spmv_policy", self.lib.sa_get_spmv_policy(self.h, C.byref(packed), C.byref(mag), C.byref(hub)))
+        return {"packed_columns": bool(packed.value), "magnitude": mag.value, "hub_columns": int(hub.value)}
+
     # ---- one alpha --------------------------------------------------------------------------
     def alpha_solve(self, *, alpha, alpha_prev, rho, gershgorin, tol, pred_tol, maxiter, ncv, start_mode,
                     seed, stream_id, align=True, v0: Optional[torch.Tensor] = None, secant_gamma=1.0,

@@ -147,11 +147,13 @@ int sa_get_spmv_policy(sa_handle* h, int32_t* packed_columns, double* magnitude,
 
 /* Column-panel SpMV. Every CTA keeps the row sums of a block of rows in shared memory and gathers
  * the scaled input from panels of it staged in shared memory, instead of from L2: it pays when
- * rows average more than ~20 entries. sa_panel_workspace_size gives the bytes of the layout for
- * the bound matrix; sa_panel_build lays the matrix out in that caller-owned device workspace
+ * rows average more than ~20 entries and the row blocks (at most 16384 rows in FP32, 8192 in
+ * FP64, about equal entries) are no more than the SMs. sa_panel_workspace_size gives the bytes of
+ * the layout for the bound matrix and its number of row blocks (row_blocks may be NULL);
+ * sa_panel_build lays the matrix out in that caller-owned device workspace
  * (256-byte aligned, kept until the next sa_set_matrix) and switches the operator kernels to it;
  * sa_panel_enable(h, 0 / 1) switches back and forth. sa_set_matrix drops the layout. */
-int sa_panel_workspace_size(sa_handle* h, size_t* bytes);
+int sa_panel_workspace_size(sa_handle* h, size_t* bytes, int32_t* row_blocks);
 int sa_panel_build(sa_handle* h, void* workspace, size_t bytes);
 int sa_panel_enable(sa_handle* h, int32_t on);
 

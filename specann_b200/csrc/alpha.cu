@@ -3,6 +3,9 @@
 
 namespace sa {
 
+PanelArgs panel_args(const sa_handle* h);
+double panel_alg_bytes(const sa_handle* h);
+
 template <typename T, typename RP>
 __global__ void __launch_bounds__(kThreads, 1) alpha_kernel(AlphaArgs<T, RP> A) {
   alpha_body<T, RP>(A, GridPolicy{});
@@ -49,9 +52,25 @@ static int launch_alpha(sa_handle* h, const sa_alpha_params* p) {
   A.group = h->group;
   A.dense = h->dense;
   A.spmv_bytes = (double)h->nnz * (4.0 + sizeof(T)) + (double)(h->n + 1) * sizeof(RP) + 3.0 * (double)h->n * sizeof(T);
+  A.use_panel = h->panel_on ? 1 : 0;
+  int dyn = 0;
+  if (A.use_panel) {
+    A.panel = panel_args(h);
+    A.spmv_bytes = panel_alg_bytes(h) + 3.0 * (double)h->n * sizeof(T);
+    dyn = panel_smem_bytes((int)sizeof(T));
+    static bool attr_set = false;
+    if (!attr_set) {
+      if (cudaFuncSetAttribute((const void*)alpha_kernel<T, RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) !=
+          cudaSuccess)
+        return SA_ERR_CUDA;
+      attr_set = true;
+    }
+  } else {
+    A.panel = PanelArgs{};
+  }
   void* args[] = {&A};
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)alpha_kernel<T, RP>, dim3(h->blocks),
-                                              dim3(kThreads), args, 0, h->stream);
+                                              dim3(kThreads), args, (size_t)dyn, h->stream);
   count_launches(1);
   return e == cudaSuccess ? SA_OK : SA_ERR_CUDA;
 }

@@ -18,6 +18,7 @@
 #include "common.cuh"
 #include "handle.cuh"
 #include "spmv.cuh"
+#include "panel.cuh"
 #include "policy.cuh"
 
 namespace sa {
@@ -58,6 +59,8 @@ struct AlphaArgs {
   int group;
   double spmv_bytes;     // algorithmic bytes of one fused SpMV
   double* dense;         // implicit-restart scratch (dense T, then dense Q)
+  PanelArgs panel;       // column-panel layout of the operator (use_panel = 1; needs
+  int use_panel;         // panel_smem_bytes(sizeof(T)) of dynamic shared memory), else the work list
 };
 
 // ---- small dense helpers for the projected tridiagonal (double, one CTA) --------------------
@@ -417,15 +420,25 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
   __shared__ double s_theta, s_s2;
   __shared__ SpmvSmem<T, NW> ssp;
   __shared__ double sq[kNcvMax * (kRestartMax + 1)];
+  __shared__ unsigned long long pbars[kPanelBufs];
+  extern __shared__ __align__(128) char panel_smem[];
   AlphaCtrl* C = A.ctrl;
   const long long n = A.n;
   const long long gtid = pol.tid();
   const long long nthreads = pol.nthr();
-  const long long gwarp = gtid >> 5, nwarps = nthreads >> 5;
   const sa_alpha_params& P = A.p;
   const double rho = P.rho;
   const double bound = 10.0 * (P.rho + P.gershgorin);
   const int ncv = P.ncv;
+  unsigned ppar = 0;   // phase bits of the panel barriers
+  if (A.use_panel) panel_init(pbars);
+  // one operator application: fin(row, sum_j val_ij u_j) once per row; false on a timed-out wait
+  auto apply = [&](auto&& fin) -> bool {
+    if (A.use_panel)
+      return panel_spmv<T>(A.panel, A.u, pol.block(), pol.nblocks(), panel_smem, pbars, ppar, &C->gs.error, fin);
+    spmv_items<T, RP>(A.S, A.u, gtid >> 5, nthreads >> 5, ssp, fin);
+    return true;
+  };
 
   // phase timer: CTA 0 thread 0 charges the time since the previous barrier exit to a phase
   unsigned long long t_mark = (pol.block() == 0 && threadIdx.x == 0) ? global_ns() : 0ull;
@@ -568,14 +581,14 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
         T* Vj = A.V + (long long)j * A.ldv;
         const T trho = (T)rho;
         double pa[1] = {0.0};
-        spmv_items<T, RP>(A.S, A.u, gwarp, nwarps, ssp, [&](long long r, T acc) {
-          const T wr = __ldcg(A.w + r);
-          const T vr = wr * inv_b;
-          const T wn = (trho * wr - __ldcg(A.sigma + r) * acc) * inv_b;
-          Vj[r] = vr;
-          A.w[r] = wn;
-          pa[0] += (double)vr * (double)wn;
-        });
+        if (!apply([&](long long r, T acc) {
+              const T wr = __ldcg(A.w + r);
+              const T vr = wr * inv_b;
+              const T wn = (trho * wr - __ldcg(A.sigma + r) * acc) * inv_b;
+              Vj[r] = vr;
+              A.w[r] = wn;
+              pa[0] += (double)vr * (double)wn;
+            })) return;
         block_store_partials<1>(pa, A.part, A.pw, 0, sm, pol.block());
         if (!pol.sync(&C->gs, [&] {
               reduce_partials(A.part, A.pw, pol.nblocks(), 1, sm);
@@ -900,13 +913,13 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
     double v[1] = {0.0};
     if (P.residual_check) {
       const T trho = (T)rho;
-      spmv_items<T, RP>(A.S, A.u, gwarp, nwarps, ssp, [&](long long r, T acc) {
-        const T yt = __ldcg(A.yout + r);
-        const double yr = (double)yt;
-        const double sy = (double)(trho * yt - __ldcg(A.sigma + r) * acc);
-        const double rr = sy - theta * yr;
-        v[0] += rr * rr;
-      });
+      if (!apply([&](long long r, T acc) {
+            const T yt = __ldcg(A.yout + r);
+            const double yr = (double)yt;
+            const double sy = (double)(trho * yt - __ldcg(A.sigma + r) * acc);
+            const double rr = sy - theta * yr;
+            v[0] += rr * rr;
+          })) return;
     }
     if (P.round) {
       const long long nr = (n + 31) & ~31ll;

@@ -106,6 +106,7 @@ struct sa_handle {
   // column-panel SpMV (sa_panel_build): layout in the caller's panel workspace
   int panel_ready = 0, panel_on = 0;
   int panel_blocks = 0, panel_count = 0, panel_width = 0;
+  long long panel_slots = 0;   // entry slots of the layout (padding included)
   const unsigned int* panel_ent = nullptr;
   const void* panel_val = nullptr;
   const long long* panel_chunk = nullptr;

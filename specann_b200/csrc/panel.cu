@@ -37,7 +37,7 @@ struct PanelPlan {
 int plan_panels(const sa_handle* h, const std::vector<long long>& rp, PanelPlan* pl) {
   const size_t T = h->prec == 32 ? 4 : 8;
   const long long max_rows = std::min<long long>(kPanelRowBytes / (long long)T, 65535);
-  pl->width = (int)(kPanelBytes / T);
+  pl->width = (int)(panel_buf_bytes((int)T) / T);
   pl->n_panels = (int)((h->n + pl->width - 1) / pl->width);
   const long long want = std::max(1, h->sm_count);
   const double target = (double)h->nnz / (double)want;
@@ -110,6 +110,17 @@ PanelArgs panel_args(const sa_handle* h) {
   return P;
 }
 
+// Algorithmic bytes of one panel SpMV read from DRAM: the entry stream (padding included), the
+// values when they differ in magnitude, the chunk bounds and the block rows. The staged input is
+// read from L2 by every CTA and counted once with the vectors by the caller.
+double panel_alg_bytes(const sa_handle* h) {
+  const double T = h->prec == 32 ? 4.0 : 8.0;
+  double b = 4.0 * (double)h->panel_slots + 16.0 * (double)h->panel_blocks * h->panel_count * kWarps +
+             4.0 * (double)(h->panel_blocks + 1);
+  if (h->panel_val) b += T * (double)h->panel_slots;
+  return b;
+}
+
 // The standalone operator through the panel layout (sa_spmv_scaled when the panel SpMV is on).
 int panel_spmv_launch(sa_handle* h, const void* u, const void* x, const void* sigma, double rho, void* y) {
   static bool attr_set[2] = {false, false};
@@ -120,18 +131,18 @@ int panel_spmv_launch(sa_handle* h, const void* u, const void* x, const void* si
   if (h->prec == 32) {
     auto k = panel_spmv_kernel<float, int>;
     if (!attr_set[0]) {
-      PN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmem));
+      PN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_smem_bytes(4)));
       attr_set[0] = true;
     }
-    k<<<grid, kThreads, kPanelSmem, h->stream>>>(P, (const float*)u, (const float*)x, (const float*)sigma, (float)rho,
+    k<<<grid, kThreads, panel_smem_bytes(4), h->stream>>>(P, (const float*)u, (const float*)x, (const float*)sigma, (float)rho,
                                                  (float*)y, err);
   } else {
     auto k = panel_spmv_kernel<double, int>;
     if (!attr_set[1]) {
-      PN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmem));
+      PN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_smem_bytes(8)));
       attr_set[1] = true;
     }
-    k<<<grid, kThreads, kPanelSmem, h->stream>>>(P, (const double*)u, (const double*)x, (const double*)sigma, rho,
+    k<<<grid, kThreads, panel_smem_bytes(8), h->stream>>>(P, (const double*)u, (const double*)x, (const double*)sigma, rho,
                                                  (double*)y, err);
   }
   count_launches(1);
@@ -143,7 +154,7 @@ int panel_spmv_launch(sa_handle* h, const void* u, const void* x, const void* si
 
 extern "C" {
 
-int sa_panel_workspace_size(sa_handle* h, size_t* bytes) {
+int sa_panel_workspace_size(sa_handle* h, size_t* bytes, int32_t* row_blocks) {
   if (!h || !h->bound || !bytes) return SA_ERR_INVALID_ARG;
   std::vector<long long> rp;
   int st = host_rowptr(h, rp);
@@ -152,6 +163,7 @@ int sa_panel_workspace_size(sa_handle* h, size_t* bytes) {
   st = plan_panels(h, rp, &pl);
   if (st != SA_OK) return st;
   *bytes = pl.total;
+  if (row_blocks) *row_blocks = (int32_t)(pl.row0.size() - 1);
   return SA_OK;
 }
 
@@ -241,6 +253,7 @@ int sa_panel_build(sa_handle* h, void* workspace, size_t bytes) {
   h->panel_chunk = (const long long*)(base + pl.off_chunk);
   h->panel_row0 = (const int*)(base + pl.off_row0);
   h->panel_blocks = nb;
+  h->panel_slots = out;
   h->panel_count = np;
   h->panel_width = width;
   h->panel_ready = 1;

@@ -3,7 +3,7 @@
 // A random 4-byte gather from global memory costs one L1 tag wavefront per lane, so the work-list
 // SpMV is bound by the L1TEX pipe (about 0.7 gathers per SM per clock on a Barabasi-Albert graph).
 // Here each CTA owns a block of rows whose partial sums live in shared memory, and walks the
-// columns in panels: panel p of the scaled input (kPanelBytes, `width` columns) is staged in shared
+// columns in panels: panel p of the scaled input (panel_buf_bytes, `width` columns) is staged in shared
 // memory by one bulk asynchronous copy (completion on an mbarrier, double-buffered so the copy of
 // panel p + 1 overlaps the work on panel p), and the block's entries with a column in panel p are
 // gathered from it. A random shared-memory gather of a warp costs about 3.5 wavefronts instead of
@@ -27,10 +27,12 @@
 
 namespace sa {
 
-constexpr int kPanelBytes = 64 * 1024;      // one staged panel of the scaled input
 constexpr int kPanelBufs = 2;               // panels in flight
 constexpr int kPanelRowBytes = 64 * 1024;   // row sums of one block
-constexpr int kPanelSmem = kPanelBufs * kPanelBytes + kPanelRowBytes;
+// One staged panel of the scaled input: 64 KB in FP32, 48 KB in FP64 (the FP64 kernels hold more
+// static shared memory); the dynamic shared memory of a panel kernel is the buffers + the row sums.
+__host__ __device__ constexpr int panel_buf_bytes(int elem) { return elem == 4 ? 64 * 1024 : 48 * 1024; }
+__host__ __device__ constexpr int panel_smem_bytes(int elem) { return kPanelBufs * panel_buf_bytes(elem) + kPanelRowBytes; }
 constexpr unsigned long long kPanelSpinLimit = 1ull << 22;   // bounded wait for a panel copy
 
 struct PanelArgs {
@@ -97,7 +99,8 @@ template <typename T>
 __device__ __forceinline__ void panel_issue(const PanelArgs& P, const T* u, int p, char* smem,
                                             unsigned long long* bars) {
   const int buf = p % kPanelBufs;
-  panel_fill(smem + (size_t)buf * kPanelBytes, u + (long long)p * P.width, panel_bytes<T>(P, p), &bars[buf]);
+  panel_fill(smem + (size_t)buf * panel_buf_bytes(sizeof(T)), u + (long long)p * P.width, panel_bytes<T>(P, p),
+             &bars[buf]);
 }
 
 // A batch is 256 entries of a warp's chunk: lane l takes the 8 consecutive entries
@@ -188,7 +191,7 @@ __device__ __forceinline__ void panel_batch(const unsigned (&r)[kPanelLane], con
 }
 
 // One SpMV over the blocks of this CTA (b = blk, blk + nblk, ...): fin(row, sum) once per row with
-// sum = sum_j val_ij u_j. smem: kPanelSmem dynamic bytes (panel buffers, then the row sums); bars:
+// sum = sum_j val_ij u_j. smem: panel_smem_bytes(sizeof(T)) dynamic bytes (panel buffers, then the row sums); bars:
 // kPanelBufs mbarriers set up by panel_init; par: the barriers' phase bits (one bit per buffer,
 // kept by the caller across calls; every thread holds the same value). Returns false, with
 // SA_ERR_BARRIER_TIMEOUT in *err, if a panel copy does not complete in time.
@@ -197,7 +200,7 @@ __device__ __forceinline__ bool panel_spmv(const PanelArgs& P, const T* u, int b
                                            unsigned long long* bars, unsigned& par, int* err, Fin&& fin) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const unsigned long long pol = l2_policy_evict_first();
-  T* ys = (T*)(smem + (size_t)kPanelBufs * kPanelBytes);
+  T* ys = (T*)(smem + (size_t)kPanelBufs * panel_buf_bytes(sizeof(T)));
   const bool uniform = P.val == nullptr;
   const T wmag = (T)P.wmag;
   const T* val = (const T*)P.val;
@@ -232,7 +235,7 @@ __device__ __forceinline__ bool panel_spmv(const PanelArgs& P, const T* u, int b
         }
       }
       par ^= 1u << buf;
-      const T* xs = (const T*)(smem + (size_t)buf * kPanelBytes);
+      const T* xs = (const T*)(smem + (size_t)buf * panel_buf_bytes(sizeof(T)));
       for (long long e = cs;; e += kPanelBatchEntries) {
         const bool more = e + kPanelBatchEntries < ce;
         unsigned nx[kPanelLane];

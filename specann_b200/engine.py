@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 from dataclasses import dataclass
-from typing import Optional
+from typing import Optional, Tuple
 
 import numpy as np
 import torch
@@ -112,11 +112,25 @@ class Engine:
         check("sa_set_spmv_policy", self.lib.sa_set_spmv_policy(self.h, 1 if packed_columns else 0,
                                                                 int(hub_columns)))
 
+    def panel_plan(self) -> Tuple[int, int]:
+        """(bytes, row blocks) of the column-panel layout of the bound matrix."""
+        nb, blocks = C.c_size_t(0), C.c_int32(0)
+        check("sa_panel_workspace_size", self.lib.sa_panel_workspace_size(self.h, C.byref(nb), C.byref(blocks)))
+        return int(nb.value), int(blocks.value)
+
+    def panels_pay(self) -> bool:
+        """The column-panel SpMV is chosen when rows average at least 16 entries and every SM
+        holds one row block."""
+        if self.n < 4096 or self.nnz < 16 * self.n:
+            return False
+        sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+        return self.panel_plan()[1] <= sms
+
     def build_panels(self) -> int:
         """Lay the bound matrix out for the column-panel SpMV (a device workspace owned by this
         engine until the next bind) and switch the operator kernels to it. Returns its bytes."""
         nb = C.c_size_t(0)
-        check("sa_panel_workspace_size", self.lib.sa_panel_workspace_size(self.h, C.byref(nb)))
+        check("sa_panel_workspace_size", self.lib.sa_panel_workspace_size(self.h, C.byref(nb), None))
         self._panel_ws = torch.empty(max(256, nb.value), dtype=torch.uint8, device=self.device)
         check("sa_panel_build", self.lib.sa_panel_build(self.h, C.c_void_p(self._panel_ws.data_ptr()),
                                                         C.c_size_t(self._panel_ws.numel())))

@@ -163,6 +163,11 @@ class SpectralAnnealing:
         self.tangent_tol = float(kwargs.pop("tangent_tol", 1e-2))
         # Ritz vectors kept by an implicit restart of the Lanczos basis (0: the kernel's default, 8)
         self.restart_keep = int(kwargs.pop("restart_keep", 0))
+        # operator layout: "auto" (column panels when rows average >= 16 entries and the row
+        # blocks fit the SMs, else the work list), "panel" or "worklist"
+        self.spmv = str(kwargs.pop("spmv", "auto"))
+        if self.spmv not in ("auto", "panel", "worklist"):
+            raise ValueError(f"spmv must be 'auto', 'panel' or 'worklist', got {self.spmv!r}")
         # local-search pass semantics: "priority" (independent flips, monotone) or "snapshot"
         self.ls_semantics = str(kwargs.pop("ls_semantics", "priority"))
         if self.ls_semantics not in ("priority", "snapshot"):
@@ -239,6 +244,7 @@ class SpectralAnnealing:
         eng = self._make_engine(n, Jc.nnz)
         data = Jc.data.astype(np.float32, copy=False) if (self.precision == 32) else Jc.data
         info = eng.upload_csr(Jc.indptr, Jc.indices, data)
+        self._choose_operator(eng)
         return self._sweep(eng, info, Jc, start_time)
 
     def solve_device(self, rowptr, col, val):
@@ -250,7 +256,16 @@ class SpectralAnnealing:
         n = int(rowptr.numel()) - 1
         eng = self._make_engine(n, int(col.numel()))
         info = eng.bind(rowptr, col, val)
+        self._choose_operator(eng)
         return self._sweep(eng, info, None, start_time)
+
+    def _choose_operator(self, eng):
+        """Lay the operator out as column panels (spmv 'panel', or 'auto' when they pay) or keep
+        the CSR work list."""
+        self.operator_layout = "worklist"
+        if self.spmv == "panel" or (self.spmv == "auto" and eng.panels_pay()):
+            eng.build_panels()
+            self.operator_layout = "panel"
 
     def _check_runnable(self):
         if self.alpha is not None:

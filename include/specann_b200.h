@@ -156,6 +156,11 @@ int sa_get_spmv_policy(sa_handle* h, int32_t* packed_columns, double* magnitude,
 int sa_panel_workspace_size(sa_handle* h, size_t* bytes, int32_t* row_blocks);
 int sa_panel_build(sa_handle* h, void* workspace, size_t bytes);
 int sa_panel_enable(sa_handle* h, int32_t on);
+/* The built layout: entry slots (padding included), row blocks, panels, columns per panel and the
+ * algorithmic DRAM bytes of one panel SpMV's matrix stream (entries, values when they differ in
+ * magnitude, chunk bounds). Any pointer may be NULL; INVALID_ARG when no layout is built. */
+int sa_panel_info(sa_handle* h, int64_t* slots, int32_t* row_blocks, int32_t* panels, int32_t* width,
+                  double* alg_bytes);
 
 /* One alpha of the sweep (models/spectral_annealing.py:568-669 with utils/eigsh.py:10-17 and
  * utils/predictors.py): start vector / predictor with its residual test, warm-started

@@ -1,9 +1,16 @@
-// Column-panel SpMV layout builder (host) and the standalone panel operator kernel.
+// Column-panel SpMV: the layout builder (on the device) and the standalone panel operator kernel.
 //
 // sa_panel_workspace_size / sa_panel_build lay the bound matrix out as panel segments (see
 // panel.cuh) in a caller-owned workspace; sa_panel_enable switches the handle's operator kernels to
-// the panel SpMV. The builder reads the CSR back to the host once and sorts it by (block, panel)
-// with a counting sort (O(nnz)).
+// the panel SpMV. The row blocks are cut on the host from the row pointers (a binary search per
+// block); everything per entry runs on the device in five launches:
+//   1. pl_words: each entry's 32-bit word (row in block, sign, column in panel), in CSR order;
+//   2. pl_sort: per block, a stable counting sort of the words by panel (one CTA per block, 512
+//      entries per round in CSR order; ranks from warp match-any and per-warp panel counts);
+//   3. pl_split: every segment cut at row boundaries into kWarps chunks of about equal length;
+//   4. pl_scan: the chunks' padded offsets (one CTA);
+//   5. pl_copy: the chunks copied to their padded slots, padding words appended.
+// The layout is a deterministic function of the CSR (stable sort, fixed cut rule).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -26,42 +33,60 @@ namespace {
     if (e_ != cudaSuccess) return SA_ERR_CUDA; \
   } while (0)
 
+constexpr int kPlMaxPanels = 256;   // panels the device builder supports (smem of pl_sort)
+
 struct PanelPlan {
   std::vector<int> row0;   // block first rows (n_blocks + 1)
   int n_panels = 0, width = 0;
-  size_t cap = 0;   // entry slots, padding included
-  size_t off_ent = 0, off_val = 0, off_chunk = 0, off_row0 = 0, total = 0;
+  long long chunks = 0;    // n_blocks * n_panels * kWarps
+  size_t cap = 0;          // entry slots, padding included (upper bound)
+  // final layout
+  size_t off_ent = 0, off_val = 0, off_chunk = 0, off_row0 = 0;
+  // build scratch
+  size_t off_w = 0, off_ws = 0, off_vs = 0, off_seg = 0, off_cs = 0, off_cl = 0, off_psz = 0;
+  size_t total = 0;
 };
 
-// Row blocks of about nnz / blocks entries and at most max_rows rows; column panels of `width`.
+// Row blocks of about nnz / SMs entries and at most max_rows rows (block b ends at the first row
+// whose entry offset reaches (b + 1) nnz / SMs, or after max_rows rows); panels of `width` columns.
 int plan_panels(const sa_handle* h, const std::vector<long long>& rp, PanelPlan* pl) {
   const size_t T = h->prec == 32 ? 4 : 8;
   const long long max_rows = std::min<long long>(kPanelRowBytes / (long long)T, 65535);
   pl->width = (int)(panel_buf_bytes((int)T) / T);
   pl->n_panels = (int)((h->n + pl->width - 1) / pl->width);
-  const long long want = std::max(1, h->sm_count);
-  const double target = (double)h->nnz / (double)want;
-  pl->row0.clear();
-  pl->row0.push_back(0);
+  if (pl->n_panels > kPlMaxPanels) return SA_ERR_INVALID_ARG;
+  const double target = (double)h->nnz / (double)std::max(1, h->sm_count);
+  pl->row0.assign(1, 0);
   long long start = 0;
   int b = 0;
   while (start < h->n) {
-    // close the block when it reaches its share of the entries or max_rows rows
     const double goal = target * (double)(b + 1);
-    long long end = start + 1;
-    while (end < h->n && end - start < max_rows && (double)rp[end] < goal) ++end;
+    // first row index in [start + 1, n) whose offset reaches the goal, else n
+    const long long idx =
+        std::lower_bound(rp.begin() + start + 1, rp.begin() + h->n, goal,
+                         [](long long v, double g) { return (double)v < g; }) - rp.begin();
+    const long long end = std::min(std::min(idx, start + max_rows), h->n);
     pl->row0.push_back((int)end);
     start = end;
     ++b;
   }
   const long long nb = (long long)pl->row0.size() - 1;
+  pl->chunks = nb * pl->n_panels * kWarps;
+  pl->cap = (size_t)std::max(1ll, h->nnz) + (size_t)(kPanelLane - 1) * (size_t)pl->chunks;
+  const bool uniform = h->wmag > 0.0;
+  const size_t nz = (size_t)std::max(1ll, h->nnz);
   Layout L;
-  // every chunk is padded to a multiple of kPanelLane entries
-  pl->cap = (size_t)std::max(1ll, h->nnz) + (size_t)(kPanelLane - 1) * (size_t)nb * pl->n_panels * kWarps;
   pl->off_ent = L.off(4 * pl->cap);
-  pl->off_val = (h->wmag > 0.0) ? 0 : L.off(T * pl->cap);
-  pl->off_chunk = L.off(8 * ((size_t)nb * pl->n_panels * kWarps + 1));
+  pl->off_val = uniform ? 0 : L.off(T * pl->cap);
+  pl->off_chunk = L.off(8 * ((size_t)pl->chunks + 1));
   pl->off_row0 = L.off(4 * (size_t)(nb + 1));
+  pl->off_w = L.off(4 * nz);
+  pl->off_ws = L.off(4 * nz);
+  pl->off_vs = uniform ? 0 : L.off(T * nz);
+  pl->off_seg = L.off(4 * (size_t)nb * pl->n_panels);
+  pl->off_cs = L.off(8 * (size_t)pl->chunks);
+  pl->off_cl = L.off(4 * (size_t)pl->chunks);
+  pl->off_psz = L.off(4 * (size_t)pl->chunks);
   pl->total = L.total;
   return SA_OK;
 }
@@ -77,6 +102,191 @@ int host_rowptr(const sa_handle* h, std::vector<long long>& rp) {
     PN_CUDA(cudaStreamSynchronize(h->stream));
     for (long long i = 0; i <= h->n; ++i) rp[i] = r32[i];
   }
+  return SA_OK;
+}
+
+// ---- device builder ------------------------------------------------------------------------
+
+// 1. words in CSR order; a warp per row
+template <typename T, typename RP>
+__global__ void pl_words(const RP* rp, const int* col, const T* val, long long n, const int* row0, int nb, int width,
+                         unsigned* W) {
+  const int lane = threadIdx.x & 31;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
+    int lo = 0, hi = nb;   // row0[lo] <= r < row0[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(row0 + mid) <= r) lo = mid;
+      else hi = mid;
+    }
+    const unsigned rl = (unsigned)(r - __ldg(row0 + lo)) << 16;
+    const long long b = rp_load(rp, r), e = rp_load(rp, r + 1);
+    for (long long k = b + lane; k < e; k += 32) {
+      const int c = __ldg(col + k);
+      W[k] = rl | ((__ldg(val + k) < T(0)) ? 0x8000u : 0u) | (unsigned)(c % width);
+    }
+  }
+}
+
+// 2. stable counting sort of one block's words by panel (CTA b = block b, kThreads threads)
+template <typename T, typename RP>
+__global__ void __launch_bounds__(kThreads) pl_sort(const RP* rp, const int* col, const T* val, const unsigned* W,
+                                                    const int* row0, int np, int width, int with_val, unsigned* Ws,
+                                                    T* Vs, int* seg_len) {
+  __shared__ int run[kPlMaxPanels];
+  __shared__ int wcnt[kWarps][kPlMaxPanels];
+  const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const long long e0 = rp_load(rp, __ldg(row0 + b)), e1 = rp_load(rp, __ldg(row0 + b + 1));
+  for (int p = tid; p < np; p += blockDim.x) run[p] = 0;
+  __syncthreads();
+  for (long long k = e0 + tid; k < e1; k += blockDim.x) atomicAdd(&run[__ldg(col + k) / width], 1);
+  __syncthreads();
+  if (tid == 0) {
+    int s = 0;
+    for (int p = 0; p < np; ++p) {
+      const int c = run[p];
+      seg_len[(long long)b * np + p] = c;
+      run[p] = s;
+      s += c;
+    }
+  }
+  __syncthreads();
+  const unsigned lt = (1u << lane) - 1u;
+  for (long long base = e0; base < e1; base += blockDim.x) {
+    const long long k = base + tid;
+    const bool ok = k < e1;
+    const int p = ok ? __ldg(col + k) / width : np;
+    const unsigned m = __match_any_sync(0xffffffffu, p);
+    const int rank = __popc(m & lt);
+    for (int q = lane; q < np; q += 32) wcnt[wid][q] = 0;
+    __syncwarp();
+    if (ok && rank == 0) wcnt[wid][p] = __popc(m);
+    __syncthreads();
+    int off = 0;
+    if (ok) {
+      for (int w = 0; w < wid; ++w) off += wcnt[w][p];
+      off += run[p] + rank;
+    }
+    __syncthreads();
+    for (int q = tid; q < np; q += blockDim.x) {
+      int s = 0;
+      for (int w = 0; w < kWarps; ++w) s += wcnt[w][q];
+      run[q] += s;
+    }
+    if (ok) {
+      Ws[e0 + off] = W[k];
+      if (with_val) Vs[e0 + off] = __ldg(val + k);
+    }
+    __syncthreads();
+  }
+}
+
+// offset of segment (b, p) inside block b's range, from the segment lengths
+__device__ __forceinline__ long long seg_offset(const int* seg_len, int b, int p, int np) {
+  long long s = 0;
+  for (int q = 0; q < p; ++q) s += seg_len[(long long)b * np + q];
+  return s;
+}
+
+// 3. chunk cuts of every segment at row boundaries; a thread per segment
+template <typename RP>
+__global__ void pl_split(const RP* rp, const int* row0, int nb, int np, const int* seg_len, const unsigned* Ws,
+                         long long* cs, int* cl, int* psz) {
+  const long long nseg = (long long)nb * np;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < nseg; g += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(g / np), p = (int)(g % np);
+    const long long s = rp_load(rp, __ldg(row0 + b)) + seg_offset(seg_len, b, p, np);
+    const long long len = seg_len[g];
+    const long long e = s + len;
+    long long prev = s;
+    for (int w = 0; w < kWarps; ++w) {
+      long long nxt = e;
+      if (w + 1 < kWarps) {
+        long long t = s + len * (w + 1) / kWarps;
+        if (t < prev) t = prev;
+        while (t > s && t < e && (Ws[t] >> 16) == (Ws[t - 1] >> 16)) ++t;
+        nxt = t;
+      }
+      const long long c = g * kWarps + w;
+      cs[c] = prev;
+      cl[c] = (int)(nxt - prev);
+      psz[c] = (int)((nxt - prev + kPanelLane - 1) / kPanelLane * kPanelLane);
+      prev = nxt;
+    }
+  }
+}
+
+// 4. exclusive scan of the padded chunk sizes into the chunk table (one CTA of kThreads)
+__global__ void __launch_bounds__(kThreads) pl_scan(const int* psz, long long m, long long* chunk) {
+  __shared__ long long part[kThreads];
+  const int t = threadIdx.x;
+  const long long per = (m + blockDim.x - 1) / blockDim.x;
+  const long long a = min(m, (long long)t * per), z = min(m, a + per);
+  long long s = 0;
+  for (long long i = a; i < z; ++i) s += psz[i];
+  part[t] = s;
+  __syncthreads();
+  if (t == 0) {
+    long long run = 0;
+    for (int q = 0; q < (int)blockDim.x; ++q) {
+      const long long v = part[q];
+      part[q] = run;
+      run += v;
+    }
+    chunk[m] = run;
+  }
+  __syncthreads();
+  long long run = part[t];
+  for (long long i = a; i < z; ++i) {
+    chunk[i] = run;
+    run += psz[i];
+  }
+}
+
+// 5. chunks to their padded slots; a warp per chunk
+template <typename T>
+__global__ void pl_copy(const long long* cs, const int* cl, const long long* chunk, long long m, const unsigned* Ws,
+                        const T* Vs, int with_val, unsigned* ent, T* pval) {
+  const int lane = threadIdx.x & 31;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < m; c += nw) {
+    const long long src = cs[c], dst = chunk[c];
+    const int len = cl[c];
+    const int padded = (int)(chunk[c + 1] - dst);
+    for (int j = lane; j < padded; j += 32) {
+      ent[dst + j] = (j < len) ? Ws[src + j] : kPanelPad;
+      if (with_val) pval[dst + j] = (j < len) ? Vs[src + j] : T(0);
+    }
+  }
+}
+
+template <typename T, typename RP>
+int build_on_device(sa_handle* h, const PanelPlan& pl, char* base) {
+  const int nb = (int)pl.row0.size() - 1, np = pl.n_panels;
+  const bool uniform = h->wmag > 0.0;
+  const int* row0 = (const int*)(base + pl.off_row0);
+  unsigned* W = (unsigned*)(base + pl.off_w);
+  unsigned* Ws = (unsigned*)(base + pl.off_ws);
+  T* Vs = uniform ? nullptr : (T*)(base + pl.off_vs);
+  int* seg = (int*)(base + pl.off_seg);
+  long long* cs = (long long*)(base + pl.off_cs);
+  int* cl = (int*)(base + pl.off_cl);
+  int* psz = (int*)(base + pl.off_psz);
+  long long* chunk = (long long*)(base + pl.off_chunk);
+  unsigned* ent = (unsigned*)(base + pl.off_ent);
+  T* pval = uniform ? nullptr : (T*)(base + pl.off_val);
+  const RP* rp = (const RP*)h->rowptr;
+  const T* val = (const T*)h->val;
+  const int g = h->sm_count * 4;
+  pl_words<T, RP><<<g, 256, 0, h->stream>>>(rp, h->col, val, h->n, row0, nb, pl.width, W);
+  pl_sort<T, RP><<<nb, kThreads, 0, h->stream>>>(rp, h->col, val, W, row0, np, pl.width, uniform ? 0 : 1, Ws, Vs, seg);
+  const int gs = (int)std::max(1ll, std::min<long long>(((long long)nb * np + 255) / 256, g));
+  pl_split<RP><<<gs, 256, 0, h->stream>>>(rp, row0, nb, np, seg, Ws, cs, cl, psz);
+  pl_scan<<<1, kThreads, 0, h->stream>>>(psz, pl.chunks, chunk);
+  pl_copy<T><<<g, 256, 0, h->stream>>>(cs, cl, chunk, pl.chunks, Ws, Vs, uniform ? 0 : 1, ent, pval);
+  count_launches(5);
+  PN_CUDA(cudaGetLastError());
   return SA_OK;
 }
 
@@ -134,16 +344,16 @@ int panel_spmv_launch(sa_handle* h, const void* u, const void* x, const void* si
       PN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_smem_bytes(4)));
       attr_set[0] = true;
     }
-    k<<<grid, kThreads, panel_smem_bytes(4), h->stream>>>(P, (const float*)u, (const float*)x, (const float*)sigma, (float)rho,
-                                                 (float*)y, err);
+    k<<<grid, kThreads, panel_smem_bytes(4), h->stream>>>(P, (const float*)u, (const float*)x, (const float*)sigma,
+                                                          (float)rho, (float*)y, err);
   } else {
     auto k = panel_spmv_kernel<double, int>;
     if (!attr_set[1]) {
       PN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_smem_bytes(8)));
       attr_set[1] = true;
     }
-    k<<<grid, kThreads, panel_smem_bytes(8), h->stream>>>(P, (const double*)u, (const double*)x, (const double*)sigma, rho,
-                                                 (double*)y, err);
+    k<<<grid, kThreads, panel_smem_bytes(8), h->stream>>>(P, (const double*)u, (const double*)x, (const double*)sigma,
+                                                          rho, (double*)y, err);
   }
   count_launches(1);
   PN_CUDA(cudaGetLastError());
@@ -176,88 +386,38 @@ int sa_panel_build(sa_handle* h, void* workspace, size_t bytes) {
   st = plan_panels(h, rp, &pl);
   if (st != SA_OK) return st;
   if (bytes < pl.total) return SA_ERR_OOM;
-  const long long nnz = h->nnz;
-  const size_t T = h->prec == 32 ? 4 : 8;
-  const bool uniform = h->wmag > 0.0;
-  std::vector<int> col(std::max(1ll, nnz));
-  std::vector<char> val((size_t)std::max(1ll, nnz) * T);
-  if (nnz > 0) {
-    PN_CUDA(cudaMemcpyAsync(col.data(), h->col, 4 * (size_t)nnz, cudaMemcpyDeviceToHost, h->stream));
-    PN_CUDA(cudaMemcpyAsync(val.data(), h->val, T * (size_t)nnz, cudaMemcpyDeviceToHost, h->stream));
-    PN_CUDA(cudaStreamSynchronize(h->stream));
-  }
-  auto negative = [&](long long k) {
-    if (T == 4) { float v; memcpy(&v, &val[(size_t)k * 4], 4); return v < 0.0f; }
-    double v; memcpy(&v, &val[(size_t)k * 8], 8); return v < 0.0;
-  };
-  const int nb = (int)pl.row0.size() - 1, np = pl.n_panels, width = pl.width;
-  std::vector<unsigned int> ent(pl.cap, kPanelPad);
-  std::vector<char> pv(uniform ? 0 : pl.cap * T, 0);
-  std::vector<long long> chunk((size_t)nb * np * kWarps + 1);
-  std::vector<long long> cnt(np + 1), pos(np);
-  std::vector<unsigned> seg;   // the current block's entries in segment order (unpadded)
-  std::vector<long long> src;  // their CSR positions
-  long long out = 0;           // next padded slot
-  for (int b = 0; b < nb; ++b) {
-    const long long r0 = pl.row0[b], r1 = pl.row0[b + 1];
-    const long long e0 = rp[r0], e1 = rp[r1];
-    std::fill(cnt.begin(), cnt.end(), 0);
-    for (long long k = e0; k < e1; ++k) cnt[col[k] / width + 1] += 1;
-    for (int p = 0; p < np; ++p) cnt[p + 1] += cnt[p];
-    for (int p = 0; p < np; ++p) pos[p] = cnt[p];
-    seg.assign((size_t)(e1 - e0), 0u);
-    src.assign((size_t)(e1 - e0), 0);
-    for (long long r = r0; r < r1; ++r) {
-      for (long long k = rp[r]; k < rp[r + 1]; ++k) {
-        const int c = col[k];
-        const int p = c / width;
-        const long long d = pos[p]++;
-        seg[(size_t)d] = ((unsigned)(r - r0) << 16) | (negative(k) ? 0x8000u : 0u) | (unsigned)(c - p * width);
-        src[(size_t)d] = k;
-      }
-    }
-    // each segment cut at row boundaries into kWarps chunks of about equal length; every chunk is
-    // written at a multiple of kPanelLane slots and padded to one
-    for (int p = 0; p < np; ++p) {
-      const long long s0 = cnt[p], s1 = cnt[p + 1];
-      long long cut[kWarps + 1];
-      cut[0] = s0;
-      cut[kWarps] = s1;
-      for (int w = 1; w < kWarps; ++w) {
-        long long t = s0 + (s1 - s0) * w / kWarps;
-        if (t < cut[w - 1]) t = cut[w - 1];
-        while (t > s0 && t < s1 && (seg[(size_t)t] >> 16) == (seg[(size_t)t - 1] >> 16)) ++t;
-        cut[w] = t;
-      }
-      for (int w = 0; w < kWarps; ++w) {
-        chunk[((size_t)b * np + p) * kWarps + w] = out;
-        for (long long q = cut[w]; q < cut[w + 1]; ++q, ++out) {
-          ent[(size_t)out] = seg[(size_t)q];
-          if (!uniform) memcpy(&pv[(size_t)out * T], &val[(size_t)src[(size_t)q] * T], T);
-        }
-        out = (out + kPanelLane - 1) / kPanelLane * kPanelLane;
-      }
-    }
-  }
-  chunk[(size_t)nb * np * kWarps] = out;
-  if ((size_t)out > pl.cap) return SA_ERR_OOM;
   char* base = (char*)workspace;
-  if (out > 0) PN_CUDA(cudaMemcpyAsync(base + pl.off_ent, ent.data(), 4 * (size_t)out, cudaMemcpyHostToDevice, h->stream));
-  if (!uniform && out > 0)
-    PN_CUDA(cudaMemcpyAsync(base + pl.off_val, pv.data(), T * (size_t)out, cudaMemcpyHostToDevice, h->stream));
-  PN_CUDA(cudaMemcpyAsync(base + pl.off_chunk, chunk.data(), 8 * chunk.size(), cudaMemcpyHostToDevice, h->stream));
+  h->panel_ready = h->panel_on = 0;
   PN_CUDA(cudaMemcpyAsync(base + pl.off_row0, pl.row0.data(), 4 * pl.row0.size(), cudaMemcpyHostToDevice, h->stream));
+  if (h->prec == 32) st = h->rp64 ? build_on_device<float, long long>(h, pl, base) : build_on_device<float, int>(h, pl, base);
+  else st = h->rp64 ? build_on_device<double, long long>(h, pl, base) : build_on_device<double, int>(h, pl, base);
+  if (st != SA_OK) return st;
+  long long slots = 0;
+  PN_CUDA(cudaMemcpyAsync(&slots, base + pl.off_chunk + 8 * (size_t)pl.chunks, 8, cudaMemcpyDeviceToHost, h->stream));
   PN_CUDA(cudaStreamSynchronize(h->stream));
+  if (slots < 0 || (size_t)slots > pl.cap) return SA_ERR_OOM;
+  const bool uniform = h->wmag > 0.0;
   h->panel_ent = (const unsigned int*)(base + pl.off_ent);
   h->panel_val = uniform ? nullptr : (const void*)(base + pl.off_val);
   h->panel_chunk = (const long long*)(base + pl.off_chunk);
   h->panel_row0 = (const int*)(base + pl.off_row0);
-  h->panel_blocks = nb;
-  h->panel_slots = out;
-  h->panel_count = np;
-  h->panel_width = width;
+  h->panel_blocks = (int)pl.row0.size() - 1;
+  h->panel_slots = slots;
+  h->panel_count = pl.n_panels;
+  h->panel_width = pl.width;
   h->panel_ready = 1;
   h->panel_on = 1;
+  return SA_OK;
+}
+
+int sa_panel_info(sa_handle* h, int64_t* slots, int32_t* row_blocks, int32_t* panels, int32_t* width,
+                  double* alg_bytes) {
+  if (!h || !h->panel_ready) return SA_ERR_INVALID_ARG;
+  if (slots) *slots = h->panel_slots;
+  if (row_blocks) *row_blocks = h->panel_blocks;
+  if (panels) *panels = h->panel_count;
+  if (width) *width = h->panel_width;
+  if (alg_bytes) *alg_bytes = panel_alg_bytes(h);
   return SA_OK;
 }
 

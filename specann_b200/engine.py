@@ -136,6 +136,13 @@ class Engine:
                                                         C.c_size_t(self._panel_ws.numel())))
         return nb.value
 
+    def panel_info(self) -> dict:
+        slots, blocks, panels, width, nb = C.c_int64(0), C.c_int32(0), C.c_int32(0), C.c_int32(0), C.c_double(0.0)
+        check("sa_panel_info", self.lib.sa_panel_info(self.h, C.byref(slots), C.byref(blocks), C.byref(panels),
+                                                      C.byref(width), C.byref(nb)))
+        return {"slots": int(slots.value), "blocks": int(blocks.value), "panels": int(panels.value),
+                "width": int(width.value), "matrix_bytes": float(nb.value)}
+
     def enable_panels(self, on: bool = True) -> None:
         check("sa_panel_enable", self.lib.sa_panel_enable(self.h, 1 if on else 0))
 

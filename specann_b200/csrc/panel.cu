@@ -7,9 +7,13 @@
 //   1. pl_words: each entry's 32-bit word (row in block, sign, column in panel), in CSR order;
 //   2. pl_sort: per block, a stable counting sort of the words by panel (one CTA per block, 512
 //      entries per round in CSR order; ranks from warp match-any and per-warp panel counts);
-//   3. pl_split: every segment cut at row boundaries into kWarps chunks of about equal length;
-//   4. pl_scan: the chunks' padded offsets (one CTA);
-//   5. pl_copy: the chunks copied to their padded slots, padding words appended.
+//   3. pl_pieces (twice: count, then write): every segment, in row order, packed into pieces of
+//      at most kPanelBatchEntries entries: rows are added whole while they fit, a row longer than
+//      a piece fills whole pieces; every piece is padded to kPanelBatchEntries slots, so a warp
+//      processes exactly one piece per batch. The segment's pieces are cut into kWarps contiguous
+//      runs, one per warp (a cut never separates the pieces of one row);
+//   4. pl_scan: the pieces' offsets (one CTA);
+//   5. pl_copy: the pieces copied to their slots, padding words appended.
 // The layout is a deterministic function of the CSR (stable sort, fixed cut rule).
 #include <algorithm>
 #include <cmath>
@@ -39,11 +43,12 @@ struct PanelPlan {
   std::vector<int> row0;   // block first rows (n_blocks + 1)
   int n_panels = 0, width = 0;
   long long chunks = 0;    // n_blocks * n_panels * kWarps
+  long long max_pieces = 0;
   size_t cap = 0;          // entry slots, padding included (upper bound)
   // final layout
   size_t off_ent = 0, off_val = 0, off_chunk = 0, off_row0 = 0;
   // build scratch
-  size_t off_w = 0, off_ws = 0, off_vs = 0, off_seg = 0, off_cs = 0, off_cl = 0, off_psz = 0;
+  size_t off_w = 0, off_ws = 0, off_vs = 0, off_seg = 0, off_npc = 0, off_pbase = 0, off_pstart = 0, off_plen = 0;
   size_t total = 0;
 };
 
@@ -72,7 +77,11 @@ int plan_panels(const sa_handle* h, const std::vector<long long>& rp, PanelPlan*
   }
   const long long nb = (long long)pl->row0.size() - 1;
   pl->chunks = nb * pl->n_panels * kWarps;
-  pl->cap = (size_t)std::max(1ll, h->nnz) + (size_t)(kPanelLane - 1) * (size_t)pl->chunks;
+  // a piece that is closed before it is full is longer than kPanelBatchEntries together with the
+  // row that follows it, so a segment of L entries has at most 2 L / kPanelBatchEntries + 1 pieces
+  const long long nseg = nb * pl->n_panels;
+  pl->max_pieces = 2 * (std::max(1ll, h->nnz) / kPanelBatchEntries) + nseg + 1;
+  pl->cap = (size_t)pl->max_pieces * kPanelBatchEntries;
   const bool uniform = h->wmag > 0.0;
   const size_t nz = (size_t)std::max(1ll, h->nnz);
   Layout L;
@@ -83,10 +92,11 @@ int plan_panels(const sa_handle* h, const std::vector<long long>& rp, PanelPlan*
   pl->off_w = L.off(4 * nz);
   pl->off_ws = L.off(4 * nz);
   pl->off_vs = uniform ? 0 : L.off(T * nz);
-  pl->off_seg = L.off(4 * (size_t)nb * pl->n_panels);
-  pl->off_cs = L.off(8 * (size_t)pl->chunks);
-  pl->off_cl = L.off(4 * (size_t)pl->chunks);
-  pl->off_psz = L.off(4 * (size_t)pl->chunks);
+  pl->off_seg = L.off(4 * (size_t)nseg);
+  pl->off_npc = L.off(4 * (size_t)nseg);
+  pl->off_pbase = L.off(8 * ((size_t)nseg + 1));
+  pl->off_pstart = L.off(8 * (size_t)pl->max_pieces);
+  pl->off_plen = L.off(4 * (size_t)pl->max_pieces);
   pl->total = L.total;
   return SA_OK;
 }
@@ -189,42 +199,70 @@ __device__ __forceinline__ long long seg_offset(const int* seg_len, int b, int p
   return s;
 }
 
-// 3. chunk cuts of every segment at row boundaries; a thread per segment
-template <typename RP>
-__global__ void pl_split(const RP* rp, const int* row0, int nb, int np, const int* seg_len, const unsigned* Ws,
-                         long long* cs, int* cl, int* psz) {
+// 3. pieces of every segment; a thread per segment walks its rows. WRITE = false: count them into
+// npc; WRITE = true: record each piece (start in the sorted words, length), starting at the
+// segment's piece offset pbase, and the chunk table (warp w's first slot).
+template <bool WRITE, typename RP>
+__global__ void pl_pieces(const RP* rp, const int* row0, int nb, int np, const int* seg_len, const unsigned* Ws,
+                          int* npc, const long long* pbase, long long* pstart, int* plen, long long* chunk) {
   const long long nseg = (long long)nb * np;
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < nseg; g += (long long)gridDim.x * blockDim.x) {
     const int b = (int)(g / np), p = (int)(g % np);
     const long long s = rp_load(rp, __ldg(row0 + b)) + seg_offset(seg_len, b, p, np);
-    const long long len = seg_len[g];
-    const long long e = s + len;
-    long long prev = s;
-    for (int w = 0; w < kWarps; ++w) {
-      long long nxt = e;
-      if (w + 1 < kWarps) {
-        long long t = s + len * (w + 1) / kWarps;
-        if (t < prev) t = prev;
-        while (t > s && t < e && (Ws[t] >> 16) == (Ws[t - 1] >> 16)) ++t;
-        nxt = t;
+    const long long e = s + seg_len[g];
+    const long long base = WRITE ? pbase[g] : 0;
+    long long cnt = 0, open = -1;   // pieces so far; start of the open piece
+    int fill = 0;
+    for (long long k = s; k < e;) {
+      const unsigned row = Ws[k] >> 16;
+      long long k2 = k + 1;
+      while (k2 < e && (Ws[k2] >> 16) == row) ++k2;
+      long long left = k2 - k;
+      if (fill > 0 && fill + left > kPanelBatchEntries) {   // the row does not fit: close the piece
+        if (WRITE) { pstart[base + cnt] = open; plen[base + cnt] = fill; }
+        ++cnt;
+        fill = 0;
       }
-      const long long c = g * kWarps + w;
-      cs[c] = prev;
-      cl[c] = (int)(nxt - prev);
-      psz[c] = (int)((nxt - prev + kPanelLane - 1) / kPanelLane * kPanelLane);
-      prev = nxt;
+      while (left > 0) {
+        if (fill == 0) open = k;
+        const long long take = min(left, (long long)(kPanelBatchEntries - fill));
+        fill += (int)take;
+        k += take;
+        left -= take;
+        if (fill == kPanelBatchEntries) {
+          if (WRITE) { pstart[base + cnt] = open; plen[base + cnt] = fill; }
+          ++cnt;
+          fill = 0;
+        }
+      }
+    }
+    if (fill > 0) {
+      if (WRITE) { pstart[base + cnt] = open; plen[base + cnt] = fill; }
+      ++cnt;
+    }
+    if (!WRITE) {
+      npc[g] = (int)cnt;
+    } else {
+      // warp w starts at piece w cnt / kWarps, moved forward past pieces that continue a row
+      for (int w = 0; w < kWarps; ++w) {
+        long long t = cnt * w / kWarps;
+        while (t > 0 && t < cnt && pstart[base + t] > s &&
+               (Ws[pstart[base + t]] >> 16) == (Ws[pstart[base + t] - 1] >> 16))
+          ++t;
+        chunk[g * kWarps + w] = (base + t) * kPanelBatchEntries;
+      }
     }
   }
 }
 
-// 4. exclusive scan of the padded chunk sizes into the chunk table (one CTA of kThreads)
-__global__ void __launch_bounds__(kThreads) pl_scan(const int* psz, long long m, long long* chunk) {
+// 4. exclusive scan of the pieces per segment (one CTA of kThreads); out[m] = total
+__global__ void __launch_bounds__(kThreads) pl_scan(const int* cnt, long long m, long long* out) {
   __shared__ long long part[kThreads];
   const int t = threadIdx.x;
   const long long per = (m + blockDim.x - 1) / blockDim.x;
   const long long a = min(m, (long long)t * per), z = min(m, a + per);
   long long s = 0;
-  for (long long i = a; i < z; ++i) s += psz[i];
+  for (long long i = a; i < z; ++i) s += cnt[i];
   part[t] = s;
   __syncthreads();
   if (t == 0) {
@@ -234,27 +272,26 @@ __global__ void __launch_bounds__(kThreads) pl_scan(const int* psz, long long m,
       part[q] = run;
       run += v;
     }
-    chunk[m] = run;
+    out[m] = run;
   }
   __syncthreads();
   long long run = part[t];
   for (long long i = a; i < z; ++i) {
-    chunk[i] = run;
-    run += psz[i];
+    out[i] = run;
+    run += cnt[i];
   }
 }
 
-// 5. chunks to their padded slots; a warp per chunk
+// 5. pieces to their slots (kPanelBatchEntries each); a warp per piece
 template <typename T>
-__global__ void pl_copy(const long long* cs, const int* cl, const long long* chunk, long long m, const unsigned* Ws,
-                        const T* Vs, int with_val, unsigned* ent, T* pval) {
+__global__ void pl_copy(const long long* pstart, const int* plen, long long pieces, const unsigned* Ws, const T* Vs,
+                        int with_val, unsigned* ent, T* pval) {
   const int lane = threadIdx.x & 31;
   const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < m; c += nw) {
-    const long long src = cs[c], dst = chunk[c];
-    const int len = cl[c];
-    const int padded = (int)(chunk[c + 1] - dst);
-    for (int j = lane; j < padded; j += 32) {
+  for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < pieces; c += nw) {
+    const long long src = pstart[c], dst = c * kPanelBatchEntries;
+    const int len = plen[c];
+    for (int j = lane; j < kPanelBatchEntries; j += 32) {
       ent[dst + j] = (j < len) ? Ws[src + j] : kPanelPad;
       if (with_val) pval[dst + j] = (j < len) ? Vs[src + j] : T(0);
     }
@@ -270,22 +307,31 @@ int build_on_device(sa_handle* h, const PanelPlan& pl, char* base) {
   unsigned* Ws = (unsigned*)(base + pl.off_ws);
   T* Vs = uniform ? nullptr : (T*)(base + pl.off_vs);
   int* seg = (int*)(base + pl.off_seg);
-  long long* cs = (long long*)(base + pl.off_cs);
-  int* cl = (int*)(base + pl.off_cl);
-  int* psz = (int*)(base + pl.off_psz);
+  int* npc = (int*)(base + pl.off_npc);
+  long long* pbase = (long long*)(base + pl.off_pbase);
+  long long* pstart = (long long*)(base + pl.off_pstart);
+  int* plen = (int*)(base + pl.off_plen);
   long long* chunk = (long long*)(base + pl.off_chunk);
   unsigned* ent = (unsigned*)(base + pl.off_ent);
   T* pval = uniform ? nullptr : (T*)(base + pl.off_val);
   const RP* rp = (const RP*)h->rowptr;
   const T* val = (const T*)h->val;
   const int g = h->sm_count * 4;
+  const long long nseg = (long long)nb * np;
   pl_words<T, RP><<<g, 256, 0, h->stream>>>(rp, h->col, val, h->n, row0, nb, pl.width, W);
   pl_sort<T, RP><<<nb, kThreads, 0, h->stream>>>(rp, h->col, val, W, row0, np, pl.width, uniform ? 0 : 1, Ws, Vs, seg);
-  const int gs = (int)std::max(1ll, std::min<long long>(((long long)nb * np + 255) / 256, g));
-  pl_split<RP><<<gs, 256, 0, h->stream>>>(rp, row0, nb, np, seg, Ws, cs, cl, psz);
-  pl_scan<<<1, kThreads, 0, h->stream>>>(psz, pl.chunks, chunk);
-  pl_copy<T><<<g, 256, 0, h->stream>>>(cs, cl, chunk, pl.chunks, Ws, Vs, uniform ? 0 : 1, ent, pval);
-  count_launches(5);
+  const int gs = (int)std::max(1ll, std::min<long long>((nseg + 127) / 128, g));
+  pl_pieces<false, RP><<<gs, 128, 0, h->stream>>>(rp, row0, nb, np, seg, Ws, npc, nullptr, nullptr, nullptr, nullptr);
+  pl_scan<<<1, kThreads, 0, h->stream>>>(npc, nseg, pbase);
+  pl_pieces<true, RP><<<gs, 128, 0, h->stream>>>(rp, row0, nb, np, seg, Ws, nullptr, pbase, pstart, plen, chunk);
+  long long pieces = 0;
+  PN_CUDA(cudaMemcpyAsync(&pieces, pbase + nseg, 8, cudaMemcpyDeviceToHost, h->stream));
+  PN_CUDA(cudaStreamSynchronize(h->stream));
+  if (pieces < 0 || pieces > pl.max_pieces) return SA_ERR_OOM;
+  const long long total = pieces * kPanelBatchEntries;
+  PN_CUDA(cudaMemcpyAsync(chunk + pl.chunks, &total, 8, cudaMemcpyHostToDevice, h->stream));
+  if (pieces > 0) pl_copy<T><<<g, 256, 0, h->stream>>>(pstart, plen, pieces, Ws, Vs, uniform ? 0 : 1, ent, pval);
+  count_launches(pieces > 0 ? 6 : 5);
   PN_CUDA(cudaGetLastError());
   return SA_OK;
 }

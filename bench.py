@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--scale-precisions", default="32,64", help="--scale-run: precisions to run, in order")
     ap.add_argument("--scale-run", action="store_true",
                     help="one timed FP32 solve and one timed plain-FP64 solve of the graph, with the energy gap")
-    ap.add_argument("--spmv-layout", choices=["auto", "panel", "worklist"], default="auto",
+    ap.add_argument("--spmv-layout", choices=["auto", "panel", "split", "worklist"], default="auto",
                     help="operator layout of --spmv-only (auto: the solver's choice)")
     ap.add_argument("--spmv-only", action="store_true",
                     help="time only the standalone fused SpMV on the resident matrix (profiling runs)")
@@ -479,9 +479,11 @@ def main():
         eng.bind(d_rowptr, d_col, d_val)
         layout = args.spmv_layout
         if layout == "auto":
-            layout = "panel" if eng.panels_pay() else "worklist"
+            layout = "panel" if eng.panels_pay() else ("split" if eng.splits_pay() else "worklist")
         if layout == "panel":
             eng.build_panels()
+        elif layout == "split":
+            eng.build_splits()
         x = torch.randn(n, device=dev, dtype=torch.float32 if args.precision == 32 else torch.float64)
         y = torch.empty_like(x)
         for _ in range(args.warmup):
@@ -498,6 +500,8 @@ def main():
         sb_ = spmv_bytes(n, nnz, rp_np.itemsize, t)
         if layout == "panel":
             sb_ = eng.panel_info()["matrix_bytes"] + 3 * n * t
+        elif layout == "split":
+            sb_ = eng.split_bytes() + 3 * n * t
         hbm_, kind_ = peaks()
         print(json.dumps({"spmv_only": True, "layout": layout, "n": n, "nnz": nnz, "ms": ms_, "bytes": sb_,
                           "GBps": sb_ / ms_ / 1e6, "frac": sb_ / ms_ / 1e6 / hbm_, "peak_source": kind_}))
@@ -561,6 +565,9 @@ def main():
         # the solve's operator layout: the matrix stream of the panel layout + x, s, y
         eng.build_panels()
         sb = eng.panel_info()["matrix_bytes"] + 3 * n * t
+    elif layout == "split":
+        eng.build_splits()
+        sb = eng.split_bytes() + 3 * n * t
     x = torch.randn(n, device=dev, dtype=torch.float32 if args.precision == 32 else torch.float64)
     y = torch.empty_like(x)
     for _ in range(3):

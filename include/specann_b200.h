@@ -156,6 +156,19 @@ int sa_get_spmv_policy(sa_handle* h, int32_t* packed_columns, double* magnitude,
 int sa_panel_workspace_size(sa_handle* h, size_t* bytes, int32_t* row_blocks);
 int sa_panel_build(sa_handle* h, void* workspace, size_t bytes);
 int sa_panel_enable(sa_handle* h, int32_t on);
+/* L2 column splits, for operators whose gathered vector is larger than L2 (n > ~8 M in FP32): the
+ * columns are cut into `splits` ranges (2..8; 0: one per 48 MB of the vector) and the operator is
+ * applied as one work-list pass per range, so every pass gathers from an L2-resident slice.
+ * sa_split_workspace_size gives the bytes of the layout (and the split count used);
+ * sa_split_build builds it in a caller-owned device workspace (256-byte aligned, kept until the
+ * next sa_set_matrix) and switches the operator kernels to it (the panel layout, if any, off);
+ * sa_split_enable switches back and forth; sa_split_count reports the splits in use (0: off) and the
+ * algorithmic bytes of one split SpMV's matrix stream and partial sums (matrix_bytes may be NULL). */
+int sa_split_workspace_size(sa_handle* h, int32_t splits, size_t* bytes, int32_t* splits_used);
+int sa_split_build(sa_handle* h, int32_t splits, void* workspace, size_t bytes);
+int sa_split_enable(sa_handle* h, int32_t on);
+int sa_split_count(sa_handle* h, int32_t* splits, double* matrix_bytes);
+
 /* The built layout: entry slots (padding included), row blocks, panels, columns per panel and the
  * algorithmic DRAM bytes of one panel SpMV's matrix stream (entries, values when they differ in
  * magnitude, chunk bounds). Any pointer may be NULL; INVALID_ARG when no layout is built. */

@@ -122,6 +122,10 @@ SIGNATURES = {
     "sa_panel_workspace_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_int32)]),
     "sa_panel_build": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "sa_panel_enable": (C.c_int, [C.c_void_p, C.c_int32]),
+    "sa_split_workspace_size": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_size_t), C.POINTER(C.c_int32)]),
+    "sa_split_build": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t]),
+    "sa_split_enable": (C.c_int, [C.c_void_p, C.c_int32]),
+    "sa_split_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "sa_panel_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                 C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "sa_get_spmv_policy": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double),

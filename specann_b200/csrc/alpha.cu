@@ -5,6 +5,8 @@ namespace sa {
 
 PanelArgs panel_args(const sa_handle* h);
 double panel_alg_bytes(const sa_handle* h);
+template <typename T, typename RP>
+SpmvArgs<T, RP> split_args(const sa_handle* h, int s);
 
 template <typename T, typename RP>
 __global__ void __launch_bounds__(kThreads, 1) alpha_kernel(AlphaArgs<T, RP> A) {
@@ -67,6 +69,14 @@ static int launch_alpha(sa_handle* h, const sa_alpha_params* p) {
     }
   } else {
     A.panel = PanelArgs{};
+  }
+  A.n_splits = 0;
+  A.split_part = nullptr;
+  if (!A.use_panel && h->split_on) {
+    A.n_splits = h->n_splits;
+    for (int q = 0; q < h->n_splits; ++q) A.split[q] = split_args<T, RP>(h, q);
+    A.split_part = (T*)h->split_part;
+    A.spmv_bytes = h->split_bytes + 3.0 * (double)h->n * sizeof(T);
   }
   void* args[] = {&A};
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)alpha_kernel<T, RP>, dim3(h->blocks),

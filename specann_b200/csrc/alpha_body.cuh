@@ -61,6 +61,9 @@ struct AlphaArgs {
   double* dense;         // implicit-restart scratch (dense T, then dense Q)
   PanelArgs panel;       // column-panel layout of the operator (use_panel = 1; needs
   int use_panel;         // panel_smem_bytes(sizeof(T)) of dynamic shared memory), else the work list
+  SpmvArgs<T, RP> split[kMaxSplits];   // L2 column splits of the operator (n_splits > 0): one
+  int n_splits;                        // work-list pass per split, partial row sums in split_part
+  T* split_part;
 };
 
 // ---- small dense helpers for the projected tridiagonal (double, one CTA) --------------------
@@ -436,6 +439,19 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
   auto apply = [&](auto&& fin) -> bool {
     if (A.use_panel)
       return panel_spmv<T>(A.panel, A.u, pol.block(), pol.nblocks(), panel_smem, pbars, ppar, &C->gs.error, fin);
+    if (A.n_splits > 0) {
+      // pass s adds the row sums of split s; a barrier makes them visible to the next pass
+      for (int q = 0; q < A.n_splits; ++q) {
+        const bool first = q == 0, last = q + 1 == A.n_splits;
+        spmv_items<T, RP>(A.split[q], A.u, gtid >> 5, nthreads >> 5, ssp, [&](long long r, T acc) {
+          const T sum = first ? acc : __ldcg(A.split_part + r) + acc;
+          if (last) fin(r, sum);
+          else __stcg(A.split_part + r, sum);
+        });
+        if (!last && !pol.sync(&C->gs)) return false;
+      }
+      return true;
+    }
     spmv_items<T, RP>(A.S, A.u, gtid >> 5, nthreads >> 5, ssp, fin);
     return true;
   };

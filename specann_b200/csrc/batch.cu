@@ -278,6 +278,7 @@ __device__ bool batch_problem(const BatchArgs& B, const BTeam& tm, int p, const 
         A.S.wmag = (T)I.wmag;
         A.S.hub = I.hub;
         A.use_panel = 0;
+        A.n_splits = 0;
         A.n = n;
         A.ldv = I.ldv;
         A.sigma = (T*)tm.sigma;

@@ -34,6 +34,7 @@ using namespace sa;
 
 namespace sa {
 int panel_spmv_launch(sa_handle* h, const void* u, const void* x, const void* sigma, double rho, void* y);
+int split_spmv_launch(sa_handle* h, const void* u, const void* x, const void* sigma, double rho, void* y);
 }
 
 namespace {
@@ -230,6 +231,11 @@ int grid_for(long long work, int threads, int sm_count) {
 }
 
 // Work list (host): short segments and long-row chunks in row order.
+}  // namespace
+
+namespace sa {
+
+// SpMV work list of a CSR (host row pointers): see max_items for the bound.
 void build_items(const std::vector<long long>& rp, long long n, std::vector<WorkItem>& items,
                  std::vector<long long>& mc_base, long long* n_long_part, double* mean_short) {
   items.clear();
@@ -273,7 +279,7 @@ void build_items(const std::vector<long long>& rp, long long n, std::vector<Work
   *mean_short = short_rows ? (double)short_elems / (double)short_rows : 0.0;
 }
 
-}  // namespace
+}  // namespace sa
 
 template <typename T, typename RP>
 static void set_policy(SpmvArgs<T, RP>& S, const sa_handle* h) {
@@ -474,6 +480,7 @@ int sa_set_matrix(sa_handle* h, const void* rowptr, const int32_t* col, const vo
   SA_CUDA(cudaStreamSynchronize(h->stream));
   h->bound = true;
   h->panel_ready = h->panel_on = 0;
+  h->split_ready = h->split_on = 0;
   h->has_last = h->has_prev = false;
   if (norm_c) *norm_c = h->c;
   if (d_min) *d_min = h->dmin;
@@ -503,14 +510,14 @@ int sa_spmv_scaled(sa_handle* h, double alpha, double rho, const void* x, void* 
   const int g = grid_for(h->n, 256, h->sm_count);
   const double hl = 0.5 * std::log2(h->c);
   const int gs = h->sm_count * 2;
-  if (h->panel_on) {
+  if (h->panel_on || h->split_on) {
     if (h->prec == 32)
       scale_kernel<float><<<g, 256, 0, h->stream>>>(h->ld, h->n, alpha, hl, (const float*)x, (float*)h->sigma, (float*)h->u);
     else
       scale_kernel<double><<<g, 256, 0, h->stream>>>(h->ld, h->n, alpha, hl, (const double*)x, (double*)h->sigma, (double*)h->u);
     count_launches(1);
     SA_CUDA(cudaGetLastError());
-    return panel_spmv_launch(h, h->u, x, h->sigma, rho, y);
+    return h->panel_on ? panel_spmv_launch(h, h->u, x, h->sigma, rho, y) : split_spmv_launch(h, h->u, x, h->sigma, rho, y);
   }
   if (h->n_mc) SA_CUDA(cudaMemsetAsync(h->mc_count, 0, 4 * h->n_mc, h->stream));
   if (h->prec == 32) {

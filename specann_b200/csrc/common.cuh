@@ -17,6 +17,7 @@ constexpr int kTileIt = kSegMax / 32;     // entries per lane of a tile
 constexpr int kNcvMax = 64;               // largest Lanczos basis
 constexpr int kDotBatch = 8;              // basis vectors per register batch in the dot phase
 constexpr unsigned long long kSpinLimit = 1ull << 25;   // ~2 s of 64 ns sleeps
+constexpr int kMaxSplits = 8;             // column splits of an operator larger than L2 (split.cu)
 
 // One tile of the SpMV work list: at most kSegMax stored entries starting at e0.
 //   row >= 0: a short segment of rows [row, row + nrows);

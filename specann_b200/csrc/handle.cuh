@@ -1,5 +1,6 @@
 // Host-side handle of the SpecAnn engine and the device control blocks of its kernels.
 #pragma once
+#include <vector>
 #include <cstdint>
 #include <cstddef>
 #include <cuda_runtime.h>
@@ -82,6 +83,11 @@ inline long long max_items(long long n, long long nnz) {
 inline long long max_multichunk_rows(long long nnz) { return nnz / (kChunk + 1) + 1; }
 inline long long max_long_partials(long long nnz) { return nnz / kChunk + max_multichunk_rows(nnz) + 1; }
 
+// The SpMV work list of a CSR given its host row pointers (capi.cu): items, the partial-sum base of
+// every multi-chunk row, the partial sums they need and the mean length of the short rows.
+void build_items(const std::vector<long long>& rp, long long n, std::vector<WorkItem>& items,
+                 std::vector<long long>& mc_base, long long* n_long_part, double* mean_short);
+
 }  // namespace sa
 
 struct sa_handle {
@@ -103,6 +109,20 @@ struct sa_handle {
   int packed = 0;           // scol holds the bound matrix and the SpMV streams it
   int packed_allowed = 1;   // sa_set_spmv_policy
   int hub = 0;              // L1-resident gather columns [0, hub) (sa_set_spmv_policy)
+  // L2 column splits (sa_split_build): per split a CSR of the columns in one range and its work list
+  int split_ready = 0, split_on = 0, n_splits = 0;
+  struct Split {
+    const void* rowptr = nullptr;    // n + 1, the handle's row pointer type
+    const int32_t* col = nullptr;    // packed signed columns when the couplings have one magnitude
+    const void* val = nullptr;       // values (null with packed columns)
+    sa::WorkItem* items = nullptr;
+    long long n_items = 0, nnz = 0;
+    long long* mc_base = nullptr;
+    int* mc_count = nullptr;
+    void* long_part = nullptr;
+  } split[sa::kMaxSplits];
+  void* split_part = nullptr;        // partial row sums between the passes (n, working precision)
+  double split_bytes = 0.0;          // algorithmic bytes of one split SpMV's matrix stream
   // column-panel SpMV (sa_panel_build): layout in the caller's panel workspace
   int panel_ready = 0, panel_on = 0;
   int panel_blocks = 0, panel_count = 0, panel_width = 0;

@@ -453,6 +453,7 @@ int sa_panel_build(sa_handle* h, void* workspace, size_t bytes) {
   h->panel_width = pl.width;
   h->panel_ready = 1;
   h->panel_on = 1;
+  h->split_on = 0;
   return SA_OK;
 }
 
@@ -470,6 +471,7 @@ int sa_panel_info(sa_handle* h, int64_t* slots, int32_t* row_blocks, int32_t* pa
 int sa_panel_enable(sa_handle* h, int32_t on) {
   if (!h || (on && !h->panel_ready)) return SA_ERR_INVALID_ARG;
   h->panel_on = on ? 1 : 0;
+  if (on) h->split_on = 0;
   return SA_OK;
 }
 

@@ -143,6 +143,35 @@ class Engine:
         return {"slots": int(slots.value), "blocks": int(blocks.value), "panels": int(panels.value),
                 "width": int(width.value), "matrix_bytes": float(nb.value)}
 
+    def build_splits(self, splits: int = 0) -> int:
+        """Lay the bound matrix out as L2 column splits (0: one per 48 MB of the gathered vector)
+        and switch the operator kernels to it. Returns the number of splits."""
+        nb, used = C.c_size_t(0), C.c_int32(0)
+        check("sa_split_workspace_size", self.lib.sa_split_workspace_size(self.h, int(splits), C.byref(nb),
+                                                                          C.byref(used)))
+        self._split_ws = torch.empty(max(256, nb.value), dtype=torch.uint8, device=self.device)
+        check("sa_split_build", self.lib.sa_split_build(self.h, int(splits), C.c_void_p(self._split_ws.data_ptr()),
+                                                        C.c_size_t(self._split_ws.numel())))
+        return int(used.value)
+
+    def enable_splits(self, on: bool = True) -> None:
+        check("sa_split_enable", self.lib.sa_split_enable(self.h, 1 if on else 0))
+
+    def split_count(self) -> int:
+        k = C.c_int32(0)
+        check("sa_split_count", self.lib.sa_split_count(self.h, C.byref(k), None))
+        return int(k.value)
+
+    def split_bytes(self) -> float:
+        """Algorithmic bytes of one split SpMV's matrix stream and partial sums (0 when off)."""
+        k, b = C.c_int32(0), C.c_double(0.0)
+        check("sa_split_count", self.lib.sa_split_count(self.h, C.byref(k), C.byref(b)))
+        return float(b.value)
+
+    def splits_pay(self) -> bool:
+        """L2 column splits are chosen when the gathered vector is larger than 48 MB (a third of L2)."""
+        return self.n * (4 if self.precision == 32 else 8) > 48 * 1024 * 1024
+
     def enable_panels(self, on: bool = True) -> None:
         check("sa_panel_enable", self.lib.sa_panel_enable(self.h, 1 if on else 0))
 

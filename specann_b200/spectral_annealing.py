@@ -164,10 +164,11 @@ class SpectralAnnealing:
         # Ritz vectors kept by an implicit restart of the Lanczos basis (0: the kernel's default, 8)
         self.restart_keep = int(kwargs.pop("restart_keep", 0))
         # operator layout: "auto" (column panels when rows average >= 16 entries and the row
-        # blocks fit the SMs, else the work list), "panel" or "worklist"
+        # blocks fit the SMs; L2 column splits when the gathered vector is larger than 48 MB; else
+        # the work list), "panel", "split" or "worklist"
         self.spmv = str(kwargs.pop("spmv", "auto"))
-        if self.spmv not in ("auto", "panel", "worklist"):
-            raise ValueError(f"spmv must be 'auto', 'panel' or 'worklist', got {self.spmv!r}")
+        if self.spmv not in ("auto", "panel", "split", "worklist"):
+            raise ValueError(f"spmv must be 'auto', 'panel', 'split' or 'worklist', got {self.spmv!r}")
         # local-search pass semantics: "priority" (independent flips, monotone) or "snapshot"
         self.ls_semantics = str(kwargs.pop("ls_semantics", "priority"))
         if self.ls_semantics not in ("priority", "snapshot"):
@@ -266,6 +267,9 @@ class SpectralAnnealing:
         if self.spmv == "panel" or (self.spmv == "auto" and eng.panels_pay()):
             eng.build_panels()
             self.operator_layout = "panel"
+        elif self.spmv == "split" or (self.spmv == "auto" and eng.splits_pay()):
+            eng.build_splits()
+            self.operator_layout = "split"
 
     def _check_runnable(self):
         if self.alpha is not None:

@@ -124,7 +124,11 @@ class Engine:
         if self.n < 4096 or self.nnz < 16 * self.n:
             return False
         sms = torch.cuda.get_device_properties(self.device).multi_processor_count
-        return self.panel_plan()[1] <= sms
+        try:
+            blocks = self.panel_plan()[1]
+        except _lib.SpecAnnError:      # more panels than the layout supports
+            return False
+        return blocks <= sms
 
     def build_panels(self) -> int:
         """Lay the bound matrix out for the column-panel SpMV (a device workspace owned by this

@@ -68,8 +68,14 @@ struct AlphaArgs {
 
 // ---- small dense helpers for the projected tridiagonal (double, one CTA) --------------------
 
+// Biased exponent of a double (integer pipe: the recurrences below test signs and magnitudes on
+// the bit pattern, keeping double compares off their dependency chains).
+__device__ __forceinline__ int dexp_bits(double v) { return (int)((__double_as_longlong(v) >> 52) & 0x7FF); }
+
 // Number of eigenvalues of the tridiagonal (a, b; size m) below x: sign changes of the leading
-// principal minors det(T_k - x I), computed with the three-term recurrence and rescaling.
+// principal minors det(T_k - x I), computed with the three-term recurrence. The pair (p_k, p_k-1) is
+// rescaled by exact powers of two every 4 steps when its exponent leaves [2^-500, 2^500] (four steps
+// of entries bounded by the Gershgorin radius cannot leave the double range from there).
 __device__ inline int sturm_count(const double* a, const double* b, int m, double x) {
   double pp = 1.0, pc = a[0] - x;
   bool neg = pc < 0.0;
@@ -78,17 +84,21 @@ __device__ inline int sturm_count(const double* a, const double* b, int m, doubl
     const double pn = (a[i] - x) * pc - b[i - 1] * b[i - 1] * pp;
     pp = pc;
     pc = pn;
-    const double mag = fabs(pc);
-    if (mag > 1e200) { pc *= 1e-200; pp *= 1e-200; }
-    else if (mag < 1e-200 && fabs(pp) < 1e-200) { pc *= 1e200; pp *= 1e200; }
-    const bool nneg = (pc != 0.0) ? (pc < 0.0) : !neg;
+    const long long bits = __double_as_longlong(pc);
+    const bool nneg = ((bits << 1) != 0) ? (bits < 0) : !neg;   // a zero minor takes the opposite sign
     cnt += (nneg != neg);
     neg = nneg;
+    if ((i & 3) == 0) {
+      const int e = max(dexp_bits(pc), dexp_bits(pp));
+      if (e > 1023 + 500) { pc *= 0x1p-500; pp *= 0x1p-500; }
+      else if (e < 1023 - 500) { pc *= 0x1p500; pp *= 0x1p500; }
+    }
   }
   return cnt;
 }
 
-// s_last^2 of the unit eigenvector for eigenvalue x: -det(T_{m-1} - x) / det'(T_m - x).
+// s_last^2 of the unit eigenvector for eigenvalue x: -det(T_{m-1} - x) / det'(T_m - x) (the same
+// rescaling as sturm_count).
 __device__ inline double last_component_sq(const double* a, const double* b, int m, double x) {
   double pp = 1.0, pc = a[0] - x, dp = 0.0, dc = -1.0;
   for (int i = 1; i < m; ++i) {
@@ -96,9 +106,11 @@ __device__ inline double last_component_sq(const double* a, const double* b, int
     const double pn = (a[i] - x) * pc - bb * pp;
     const double dn = -pc + (a[i] - x) * dc - bb * dp;
     pp = pc; pc = pn; dp = dc; dc = dn;
-    const double mag = fmax(fmax(fabs(pc), fabs(dc)), fmax(fabs(pp), fabs(dp)));
-    if (mag > 1e200) { pc *= 1e-200; pp *= 1e-200; dc *= 1e-200; dp *= 1e-200; }
-    else if (mag < 1e-200 && mag > 0.0) { pc *= 1e200; pp *= 1e200; dc *= 1e200; dp *= 1e200; }
+    if ((i & 3) == 0) {
+      const int e = max(max(dexp_bits(pc), dexp_bits(dc)), max(dexp_bits(pp), dexp_bits(dp)));
+      if (e > 1023 + 500) { pc *= 0x1p-500; pp *= 0x1p-500; dc *= 0x1p-500; dp *= 0x1p-500; }
+      else if (e < 1023 - 500 && e > 0) { pc *= 0x1p500; pp *= 0x1p500; dc *= 0x1p500; dp *= 0x1p500; }
+    }
   }
   // pp = det(T_{m-1} - x) (1 for m = 1), dc = det'(T_m - x)
   if (dc == 0.0) return 1.0;

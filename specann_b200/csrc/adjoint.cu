@@ -55,6 +55,8 @@ struct AdjArgs {
   double* part;
   int pw;
   AdjCtrl* ctrl;
+  PanelArgs panel;   // column-panel layout of the operator (use_panel = 1, with
+  int use_panel;     // panel_smem_bytes(sizeof(T)) of dynamic shared memory), else the work list
 };
 
 // l_i = -1/2 ln d_i where d_i^{a_i} is above the clamp (else 0: D_i does not depend on a_i there)
@@ -72,11 +74,22 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjArgs<T, RP> A) 
   __shared__ double sm[kWarps * 4];
   __shared__ double sh[8];
   __shared__ SpmvSmem<T> ssp;
+  __shared__ unsigned long long pbars[kPanelBufs];
+  extern __shared__ __align__(128) char panel_smem[];
   const GridPolicy pol;
   AdjCtrl* C = A.ctrl;
   const long long n = A.n;
   const long long gtid = pol.tid(), nthreads = pol.nthr();
   const long long gwarp = gtid >> 5, nwarps = nthreads >> 5;
+  unsigned ppar = 0;
+  if (A.use_panel) panel_init(pbars);
+  // one operator application: fin(row, sum_j val_ij u_j) once per row; false on a timed-out wait
+  auto apply = [&](auto&& fin) -> bool {
+    if (A.use_panel)
+      return panel_spmv<T>(A.panel, A.u, pol.block(), pol.nblocks(), panel_smem, pbars, ppar, &C->gs.error, fin);
+    spmv_items<T, RP>(A.S, A.u, gwarp, nwarps, ssp, fin);
+    return true;
+  };
   const T tlam = (T)A.lambda;
 
   // ---- P0: scaling for the exponents, zero the recurrences' vectors, mode set-up ------------
@@ -111,7 +124,7 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjArgs<T, RP> A) 
   // ---- P1: right-hand side G (and the loss) ---------------------------------------------------
   if (A.mode == 0) {
     double v[2] = {0.0, 0.0};
-    spmv_items<T, RP>(A.S, A.u, gwarp, nwarps, ssp, [&](long long r, T acc) {
+    if (!apply([&](long long r, T acc) {
       const double t = (double)__ldcg(A.u + r);
       const double jt = (double)acc;
       const double gx = -A.beta_s * (1.0 - t * t) * jt;
@@ -119,7 +132,7 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjArgs<T, RP> A) 
       A.G[r] = gy;
       v[0] += t * jt;
       v[1] += (double)__ldg(A.yhat + r) * (double)gy;
-    });
+    })) return;
     block_store_partials<2>(v, A.part, A.pw, 0, sm, blockIdx.x);
     if (!grid_barrier(&C->gs, [&] {
           reduce_partials(A.part, A.pw, gridDim.x, 2, sh);
@@ -130,19 +143,19 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjArgs<T, RP> A) 
           }
         })) return;
   } else if (A.mode == 1) {
-    spmv_items<T, RP>(A.S, A.u, gwarp, nwarps, ssp, [&](long long r, T acc) {
+    if (!apply([&](long long r, T acc) {
       A.Z[r] = __ldcg(A.sigma + r) * acc;                     // (M y)_r
-    });
+    })) return;
     if (!grid_barrier(&C->gs)) return;
     for (long long i = gtid; i < n; i += nthreads)
       A.u[i] = (T)((double)__ldcg(A.sigma + i) * dlog_of(A, i) * (double)__ldg(A.yhat + i));
     if (!grid_barrier(&C->gs)) return;
     double v[1] = {0.0};
-    spmv_items<T, RP>(A.S, A.u, gwarp, nwarps, ssp, [&](long long r, T acc) {
+    if (!apply([&](long long r, T acc) {
       const T g = (T)(dlog_of(A, r) * (double)__ldcg(A.Z + r) + (double)__ldcg(A.sigma + r) * (double)acc);
       A.G[r] = g;
       v[0] += (double)__ldg(A.yhat + r) * (double)g;
-    });
+    })) return;
     block_store_partials<1>(v, A.part, A.pw, 0, sm, blockIdx.x);
     if (!grid_barrier(&C->gs, [&] {
           reduce_partials(A.part, A.pw, gridDim.x, 1, sh);
@@ -221,14 +234,14 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjArgs<T, RP> A) 
       const double fr1 = itn >= 1 ? beta / oldb : 0.0;
       const T* r1 = A.R[ir1];
       T* yv = A.R[iy];
-      spmv_items<T, RP>(A.S, A.u, gwarp, nwarps, ssp, [&](long long r, T acc) {
+      if (!apply([&](long long r, T acc) {
         const T vr = __ldcg(A.V + r);
         double y = (double)(tlam * vr - __ldcg(A.sigma + r) * acc);
         if (itn >= 1) y -= fr1 * (double)__ldcg(r1 + r);
         const T yt = (T)y;
         yv[r] = yt;
         v[0] += (double)vr * (double)yt;
-      });
+      })) return;
       block_store_partials<1>(v, A.part, A.pw, 0, sm, blockIdx.x);
       if (!grid_barrier(&C->gs, [&] {
             reduce_partials(A.part, A.pw, gridDim.x, 1, sh);
@@ -346,21 +359,21 @@ __global__ void __launch_bounds__(kThreads, 1) adjoint_kernel(AdjArgs<T, RP> A) 
   if (!grid_barrier(&C->gs)) return;
 
   // ---- gradient: M w, then M y and the assembly --------------------------------------------------
-  spmv_items<T, RP>(A.S, A.u, gwarp, nwarps, ssp, [&](long long r, T acc) {
+  if (!apply([&](long long r, T acc) {
     A.Z[r] = __ldcg(A.sigma + r) * acc;
-  });
+  })) return;
   if (!grid_barrier(&C->gs)) return;
   for (long long i = gtid; i < n; i += nthreads) A.u[i] = __ldcg(A.sigma + i) * __ldg(A.yhat + i);
   if (!grid_barrier(&C->gs)) return;
   {
     double v[1] = {0.0};
-    spmv_items<T, RP>(A.S, A.u, gwarp, nwarps, ssp, [&](long long r, T acc) {
+    if (!apply([&](long long r, T acc) {
       const double my = (double)__ldcg(A.sigma + r) * (double)acc;
       const double g = A.grad[r] + dlog_of(A, r) * ((double)__ldg(A.yhat + r) * (double)__ldcg(A.Z + r) +
                                                     (double)__ldcg(A.X + r) * my);
       A.grad[r] = g;
       v[0] += g;
-    });
+    })) return;
     block_store_partials<1>(v, A.part, A.pw, 0, sm, blockIdx.x);
     grid_barrier(&C->gs, [&] {
       reduce_partials(A.part, A.pw, gridDim.x, 1, sh);
@@ -394,6 +407,8 @@ static AdjCarve adj_carve(long long n, int prec, int blocks) {
   c.total = L.total;
   return c;
 }
+
+PanelArgs panel_args(const sa_handle* h);
 
 template <typename T, typename RP>
 static int launch_adjoint(sa_handle* h, const sa_adjoint_params* p, char* ws, int blocks) {
@@ -431,9 +446,22 @@ static int launch_adjoint(sa_handle* h, const sa_adjoint_params* p, char* ws, in
   A.ctrl = (AdjCtrl*)(ws + c.ctrl);
   if (cudaMemsetAsync(A.ctrl, 0, sizeof(GridSync), h->stream) != cudaSuccess) return SA_ERR_CUDA;
   if (h->n_mc && cudaMemsetAsync(h->mc_count, 0, 4 * h->n_mc, h->stream) != cudaSuccess) return SA_ERR_CUDA;
+  A.use_panel = h->panel_on ? 1 : 0;
+  A.panel = A.use_panel ? panel_args(h) : PanelArgs{};
+  size_t dyn = 0;
+  if (A.use_panel) {
+    dyn = (size_t)panel_smem_bytes((int)sizeof(T));
+    static bool attr_set = false;
+    if (!attr_set) {
+      if (cudaFuncSetAttribute((const void*)adjoint_kernel<T, RP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)dyn) != cudaSuccess)
+        return SA_ERR_CUDA;
+      attr_set = true;
+    }
+  }
   void* args[] = {&A};
   const cudaError_t e = cudaLaunchCooperativeKernel((const void*)adjoint_kernel<T, RP>, dim3(blocks), dim3(kThreads),
-                                                    args, 0, h->stream);
+                                                    args, dyn, h->stream);
   count_launches(1);
   return e == cudaSuccess ? SA_OK : SA_ERR_CUDA;
 }

@@ -32,6 +32,11 @@ class EigenProblem:
         self.engine = Engine(n, self.J.nnz, precision=precision, ncv_max=max(2, min(ncv, 64)), max_candidates=1)
         data = self.J.data.astype(np.float32 if precision == 32 else np.float64)
         self.info = self.engine.upload_csr(self.J.indptr, self.J.indices, data)
+        # the operator layout the solver would choose (the eigenpair and the adjoint both use it)
+        self.operator_layout = "worklist"
+        if self.engine.panels_pay():
+            self.engine.build_panels()
+            self.operator_layout = "panel"
         deg = np.asarray(abs(self.J).sum(axis=1)).ravel()
         self.d = deg / deg.max()
         self.ncv = max(2, min(ncv, n - 1, 64))

@@ -119,9 +119,10 @@ class Engine:
         return int(nb.value), int(blocks.value)
 
     def panels_pay(self) -> bool:
-        """The column-panel SpMV is chosen when rows average at least 16 entries and every SM
-        holds one row block."""
-        if self.n < 4096 or self.nnz < 16 * self.n:
+        """The column-panel SpMV is chosen in FP32 when rows average at least 16 entries and every
+        SM holds one row block (in FP64 the persistent kernels spill with its shared-memory budget
+        and the alpha solve measured slower: 15.6 against 11.5 ms on BA(2^18, 20))."""
+        if self.precision != 32 or self.n < 4096 or self.nnz < 16 * self.n:
             return False
         sms = torch.cuda.get_device_properties(self.device).multi_processor_count
         try:

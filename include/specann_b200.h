@@ -135,15 +135,13 @@ int sa_set_matrix(sa_handle* h, const void* rowptr, const int32_t* col, const vo
 int sa_spmv_scaled(sa_handle* h, double alpha, double rho, const void* x, void* y);
 
 /* SpMV stream policy (every kernel that applies the operator). packed_columns = 1 (the default):
- * when every coupling of the bound matrix has the same magnitude w, the SpMV streams one int32 per
- * entry (the column with the coupling's sign in bit 31) instead of the column and the value; the
- * products are unchanged. hub_columns = H > 0: gathers of columns below H are kept in L1, the
- * others bypass it (0, the default: one L1 policy for every gather). Takes effect at the next
- * launch and survives sa_set_matrix. */
-int sa_set_spmv_policy(sa_handle* h, int32_t packed_columns, int64_t hub_columns);
-/* The policy in effect: packed (1 when the packed stream is used), the common coupling magnitude
- * (0 when the magnitudes differ) and the hub column count. Any pointer may be NULL. */
-int sa_get_spmv_policy(sa_handle* h, int32_t* packed_columns, double* magnitude, int64_t* hub_columns);
+ * when every coupling of the bound matrix has the same magnitude w, the work-list SpMV streams one
+ * int32 per entry (the column with the coupling's sign in bit 31) instead of the column and the
+ * value; the products are unchanged. Takes effect at the next launch and survives sa_set_matrix. */
+int sa_set_spmv_policy(sa_handle* h, int32_t packed_columns);
+/* The policy in effect: packed (1 when the packed stream is used) and the common coupling magnitude
+ * (0 when the magnitudes differ). Any pointer may be NULL. */
+int sa_get_spmv_policy(sa_handle* h, int32_t* packed_columns, double* magnitude);
 
 /* Column-panel SpMV. Every CTA keeps the row sums of a block of rows in shared memory and gathers
  * the scaled input from panels of it staged in shared memory, instead of from L2: it pays when

@@ -118,7 +118,7 @@ SIGNATURES = {
     "sa_set_matrix": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
                                 C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "sa_spmv_scaled": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
-    "sa_set_spmv_policy": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64]),
+    "sa_set_spmv_policy": (C.c_int, [C.c_void_p, C.c_int32]),
     "sa_panel_workspace_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_int32)]),
     "sa_panel_build": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "sa_panel_enable": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -128,8 +128,7 @@ SIGNATURES = {
     "sa_split_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "sa_panel_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                 C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
-    "sa_get_spmv_policy": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double),
-                                     C.POINTER(C.c_int64)]),
+    "sa_get_spmv_policy": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "sa_alpha_solve": (C.c_int, [C.c_void_p, C.POINTER(AlphaParams), C.POINTER(AlphaRecord)]),
     "sa_result_vector": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "sa_commit_alpha": (C.c_int, [C.c_void_p]),

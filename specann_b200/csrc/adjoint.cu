@@ -418,7 +418,6 @@ static int launch_adjoint(sa_handle* h, const sa_adjoint_params* p, char* ws, in
                          h->mc_count, (T*)h->long_part};
   A.S.scol = h->packed ? h->scol : nullptr;
   A.S.wmag = (T)h->wmag;
-  A.S.hub = h->hub;
   A.n = h->n;
   A.ld = h->ld;
   A.aoff = h->aoff;

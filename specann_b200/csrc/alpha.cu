@@ -28,7 +28,6 @@ static int launch_alpha(sa_handle* h, const sa_alpha_params* p) {
   A.S.long_part = (T*)h->long_part;
   A.S.scol = h->packed ? h->scol : nullptr;
   A.S.wmag = (T)h->wmag;
-  A.S.hub = h->hub;
   A.n = h->n;
   A.ldv = h->ldv;
   A.sigma = (T*)h->sigma;

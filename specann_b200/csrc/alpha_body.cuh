@@ -426,8 +426,10 @@ __device__ __forceinline__ unsigned long long word_mix(long long widx, unsigned 
 // reduced columns of the dot phase (up to 2 kNcvMax + kDotBatch + 8 partial columns).
 constexpr int kRedCols = 2 * kNcvMax + kDotBatch + 8;
 
-// NW: warps per CTA at most (sizes the shared staging).
-template <typename T, typename RP, class Pol, int NW = kWarps>
+// NW: warps per CTA at most (sizes the shared staging). kLayouts: the operator may use the column-panel
+// layout or the L2 column splits (the single-problem kernel); without it only the work list is compiled
+// (the batch kernel, whose register budget the other paths would spill).
+template <typename T, typename RP, class Pol, int NW = kWarps, bool kLayouts = true>
 __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol& pol) {
   static_assert(NW * (kDotBatch + 1) <= kRedCols, "reduction scratch too small");
   __shared__ double sm[kRedCols];
@@ -446,23 +448,27 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
   const double bound = 10.0 * (P.rho + P.gershgorin);
   const int ncv = P.ncv;
   unsigned ppar = 0;   // phase bits of the panel barriers
-  if (A.use_panel) panel_init(pbars);
+  if (kLayouts && A.use_panel) panel_init(pbars);
   // one operator application: fin(row, sum_j val_ij u_j) once per row; false on a timed-out wait
   auto apply = [&](auto&& fin) -> bool {
-    if (A.use_panel)
-      return panel_spmv<T>(A.panel, A.u, pol.block(), pol.nblocks(), panel_smem, pbars, ppar, &C->gs.error, fin);
-    if (A.n_splits > 0) {
-      // pass s adds the row sums of split s; a barrier makes them visible to the next pass
-      for (int q = 0; q < A.n_splits; ++q) {
-        const bool first = q == 0, last = q + 1 == A.n_splits;
-        spmv_items<T, RP>(A.split[q], A.u, gtid >> 5, nthreads >> 5, ssp, [&](long long r, T acc) {
-          const T sum = first ? acc : __ldcg(A.split_part + r) + acc;
-          if (last) fin(r, sum);
-          else __stcg(A.split_part + r, sum);
-        });
-        if (!last && !pol.sync(&C->gs)) return false;
+    if constexpr (kLayouts) {
+      if (A.use_panel)
+        return panel_spmv<T>(A.panel, A.u, pol.block(), pol.nblocks(), panel_smem, pbars, ppar, &C->gs.error, fin);
+    }
+    if constexpr (kLayouts) {
+      if (A.n_splits > 0) {
+        // pass s adds the row sums of split s; a barrier makes them visible to the next pass
+        for (int q = 0; q < A.n_splits; ++q) {
+          const bool first = q == 0, last = q + 1 == A.n_splits;
+          spmv_items<T, RP>(A.split[q], A.u, gtid >> 5, nthreads >> 5, ssp, [&](long long r, T acc) {
+            const T sum = first ? acc : __ldcg(A.split_part + r) + acc;
+            if (last) fin(r, sum);
+            else __stcg(A.split_part + r, sum);
+          });
+          if (!last && !pol.sync(&C->gs)) return false;
+        }
+        return true;
       }
-      return true;
     }
     spmv_items<T, RP>(A.S, A.u, gtid >> 5, nthreads >> 5, ssp, fin);
     return true;

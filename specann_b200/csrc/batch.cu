@@ -51,7 +51,6 @@ struct BInstance {
   int integer_J, rp64;
   const int* scol;   // packed signed columns (one coupling magnitude wmag) or null
   double wmag;
-  int hub, pad;
 };
 
 // Sweep state of the problem a team is running (written in barrier epilogues).
@@ -276,7 +275,6 @@ __device__ bool batch_problem(const BatchArgs& B, const BTeam& tm, int p, const 
         A.S.long_part = (T*)tm.long_part;
         A.S.scol = I.scol;
         A.S.wmag = (T)I.wmag;
-        A.S.hub = I.hub;
         A.use_panel = 0;
         A.n_splits = 0;
         A.n = n;
@@ -324,7 +322,7 @@ __device__ bool batch_problem(const BatchArgs& B, const BTeam& tm, int p, const 
         A.dense = tm.dense;
       }
       __syncthreads();
-      alpha_body<T, RP, TeamPolicy, kBatchWarps>(A, pol);
+      alpha_body<T, RP, TeamPolicy, kBatchWarps, false>(A, pol);
       if (ld_volatile_i32(&pol.gs->error)) return false;
       if (pol.block() == 0 && threadIdx.x == 0)
         for (int q = 0; q < 6; ++q) pr.sum->phase_ms[q] += (double)tm.actrl->tph[q] * 1e-6;
@@ -793,8 +791,6 @@ int sa_batch_create(sa_batch** out, int32_t n_inst, sa_handle* const* inst, int3
     I.rp64 = h->rp64;
     I.scol = h->packed ? h->scol : nullptr;
     I.wmag = h->wmag;
-    I.hub = h->hub;
-    I.pad = 0;
   }
   // teams: working arrays
   char* base = b->ws + sz.header;

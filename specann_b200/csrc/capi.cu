@@ -285,7 +285,6 @@ template <typename T, typename RP>
 static void set_policy(SpmvArgs<T, RP>& S, const sa_handle* h) {
   S.scol = h->packed ? h->scol : nullptr;
   S.wmag = (T)h->wmag;
-  S.hub = h->hub;
 }
 
 extern "C" {
@@ -489,19 +488,17 @@ int sa_set_matrix(sa_handle* h, const void* rowptr, const int32_t* col, const vo
   return SA_OK;
 }
 
-int sa_set_spmv_policy(sa_handle* h, int32_t packed_columns, int64_t hub_columns) {
-  if (!h || hub_columns < 0 || (packed_columns != 0 && packed_columns != 1)) return SA_ERR_INVALID_ARG;
+int sa_set_spmv_policy(sa_handle* h, int32_t packed_columns) {
+  if (!h || (packed_columns != 0 && packed_columns != 1)) return SA_ERR_INVALID_ARG;
   h->packed_allowed = packed_columns;
   h->packed = (h->bound && h->wmag > 0.0 && packed_columns) ? 1 : 0;
-  h->hub = (int)std::min<int64_t>(hub_columns, h->n);
   return SA_OK;
 }
 
-int sa_get_spmv_policy(sa_handle* h, int32_t* packed_columns, double* magnitude, int64_t* hub_columns) {
+int sa_get_spmv_policy(sa_handle* h, int32_t* packed_columns, double* magnitude) {
   if (!h) return SA_ERR_INVALID_ARG;
   if (packed_columns) *packed_columns = h->packed;
   if (magnitude) *magnitude = h->wmag;
-  if (hub_columns) *hub_columns = h->hub;
   return SA_OK;
 }
 

@@ -108,7 +108,6 @@ struct sa_handle {
   double wmag = 0.0;        // the common |J_ij| when every coupling has it, else 0
   int packed = 0;           // scol holds the bound matrix and the SpMV streams it
   int packed_allowed = 1;   // sa_set_spmv_policy
-  int hub = 0;              // L1-resident gather columns [0, hub) (sa_set_spmv_policy)
   // L2 column splits (sa_split_build): per split a CSR of the columns in one range and its work list
   int split_ready = 0, split_on = 0, n_splits = 0;
   struct Split {

@@ -295,7 +295,6 @@ SpmvArgs<T, RP> split_args_t(const sa_handle* h, int s) {
   A.long_part = (T*)d.long_part;
   A.scol = d.val ? nullptr : d.col;
   A.wmag = (T)h->wmag;
-  A.hub = 0;
   return A;
 }
 

@@ -43,10 +43,8 @@ struct SpmvArgs {
   // when the magnitudes differ. The products are the same: val[k] is exactly +-wmag.
   const int* scol;
   T wmag;
-  // Gathers of columns below hub stay in L1 (evict_last), the others bypass it (no_allocate);
-  // 0: every gather with the default L1 policy. (No default member initialisers: the batch kernel
-  // keeps these arguments in shared memory; brace-initialised copies zero the trailing fields.)
-  int hub;
+  // (No default member initialisers: the batch kernel keeps these arguments in shared memory;
+  // brace-initialised copies zero the trailing fields.)
 };
 
 // Per-warp shared staging of a tile: kSegMax products and kSegRows + 1 row offsets, for CTAs of
@@ -110,37 +108,6 @@ __device__ __forceinline__ double ld_gather(const double* p, unsigned long long 
 template <bool kReadOnlyU, typename T>
 __device__ __forceinline__ T gather(const T* u, int j, unsigned long long pol) {
   return ld_gather(u + j, pol, kReadOnlyU);
-}
-
-// Gather with an L1 policy chosen by the column: j < hub kept in L1 (evict_last), j >= hub not
-// allocated in L1. One predicated load of each kind, so the warp's loads stay independent.
-__device__ __forceinline__ float ld_gather_hub(const float* p, int j, int hub, unsigned long long pol, bool nc) {
-  float v;
-  if (nc)
-    asm volatile("{\n .reg .pred hp;\n setp.lt.s32 hp, %2, %3;\n"
-                 " @hp ld.global.nc.L1::evict_last.L2::cache_hint.f32 %0, [%1], %4;\n"
-                 " @!hp ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %4;\n}"
-                 : "=f"(v) : "l"(p), "r"(j), "r"(hub), "l"(pol));
-  else
-    asm volatile("{\n .reg .pred hp;\n setp.lt.s32 hp, %2, %3;\n"
-                 " @hp ld.global.L1::evict_last.L2::cache_hint.f32 %0, [%1], %4;\n"
-                 " @!hp ld.global.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %4;\n}"
-                 : "=f"(v) : "l"(p), "r"(j), "r"(hub), "l"(pol));
-  return v;
-}
-__device__ __forceinline__ double ld_gather_hub(const double* p, int j, int hub, unsigned long long pol, bool nc) {
-  double v;
-  if (nc)
-    asm volatile("{\n .reg .pred hp;\n setp.lt.s32 hp, %2, %3;\n"
-                 " @hp ld.global.nc.L1::evict_last.L2::cache_hint.f64 %0, [%1], %4;\n"
-                 " @!hp ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %4;\n}"
-                 : "=d"(v) : "l"(p), "r"(j), "r"(hub), "l"(pol));
-  else
-    asm volatile("{\n .reg .pred hp;\n setp.lt.s32 hp, %2, %3;\n"
-                 " @hp ld.global.L1::evict_last.L2::cache_hint.f64 %0, [%1], %4;\n"
-                 " @!hp ld.global.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %4;\n}"
-                 : "=d"(v) : "l"(p), "r"(j), "r"(hub), "l"(pol));
-  return v;
 }
 
 struct TileDesc {
@@ -215,18 +182,10 @@ __device__ __forceinline__ void spmv_items(const SpmvArgs<T, RP>& S, const T* u,
     const TileDesc nn = load_desc(S.items, it + 2 * nwarps, S.n_items, pol_stream);
     // stage 2: the current tile
     const int len = item_len(cur.meta);
-    if (S.hub > 0) {
 #pragma unroll
-      for (int q = 0; q < kTileIt; ++q) {
-        const int k = lane + 32 * q;
-        if (k < len) v[q] *= ld_gather_hub(u + ci[q], ci[q], S.hub, pol_gather, kReadOnlyU);
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < kTileIt; ++q) {
-        const int k = lane + 32 * q;
-        if (k < len) v[q] *= gather<kReadOnlyU>(u, ci[q], pol_gather);
-      }
+    for (int q = 0; q < kTileIt; ++q) {
+      const int k = lane + 32 * q;
+      if (k < len) v[q] *= gather<kReadOnlyU>(u, ci[q], pol_gather);
     }
     if (cur.row >= 0) {
       const int nr = item_nrows(cur.meta);

@@ -106,11 +106,9 @@ class Engine:
                                                         C.c_void_p(y.data_ptr())))
         return y
 
-    def set_spmv_policy(self, packed_columns: bool = True, hub_columns: int = 0) -> None:
-        """SpMV stream policy: packed signed columns for one-magnitude couplings, and the number
-        of leading columns whose gathers stay in L1 (0: one policy for all)."""
-        check("sa_set_spmv_policy", self.lib.sa_set_spmv_policy(self.h, 1 if packed_columns else 0,
-                                                                int(hub_columns)))
+    def set_spmv_policy(self, packed_columns: bool = True) -> None:
+        """SpMV stream policy: packed signed columns for one-magnitude couplings."""
+        check("sa_set_spmv_policy", self.lib.sa_set_spmv_policy(self.h, 1 if packed_columns else 0))
 
     def panel_plan(self) -> Tuple[int, int]:
         """(bytes, row blocks) of the column-panel layout of the bound matrix."""
@@ -181,9 +179,9 @@ class Engine:
         check("sa_panel_enable", self.lib.sa_panel_enable(self.h, 1 if on else 0))
 
     def spmv_policy(self) -> dict:
-        packed, mag, hub = C.c_int32(0), C.c_double(0.0), C.c_int64(0)
-        check("sa_get_spmv_policy", self.lib.sa_get_spmv_policy(self.h, C.byref(packed), C.byref(mag), C.byref(hub)))
-        return {"packed_columns": bool(packed.value), "magnitude": mag.value, "hub_columns": int(hub.value)}
+        packed, mag = C.c_int32(0), C.c_double(0.0)
+        check("sa_get_spmv_policy", self.lib.sa_get_spmv_policy(self.h, C.byref(packed), C.byref(mag)))
+        return {"packed_columns": bool(packed.value), "magnitude": mag.value}
 
     # ---- one alpha --------------------------------------------------------------------------
     def alpha_solve(self, *, alpha, alpha_prev, rho, gershgorin, tol, pred_tol, maxiter, ncv, start_mode,

@@ -450,13 +450,10 @@ static int launch_adjoint(sa_handle* h, const sa_adjoint_params* p, char* ws, in
   size_t dyn = 0;
   if (A.use_panel) {
     dyn = (size_t)panel_smem_bytes((int)sizeof(T));
-    static bool attr_set = false;
-    if (!attr_set) {
-      if (cudaFuncSetAttribute((const void*)adjoint_kernel<T, RP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)dyn) != cudaSuccess)
-        return SA_ERR_CUDA;
-      attr_set = true;
-    }
+    // set on every launch: the attribute belongs to the current device
+    if (cudaFuncSetAttribute((const void*)adjoint_kernel<T, RP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dyn) != cudaSuccess)
+      return SA_ERR_CUDA;
   }
   void* args[] = {&A};
   const cudaError_t e = cudaLaunchCooperativeKernel((const void*)adjoint_kernel<T, RP>, dim3(blocks), dim3(kThreads),

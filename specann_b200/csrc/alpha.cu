@@ -59,13 +59,10 @@ static int launch_alpha(sa_handle* h, const sa_alpha_params* p) {
     A.panel = panel_args(h);
     A.spmv_bytes = panel_alg_bytes(h) + 3.0 * (double)h->n * sizeof(T);
     dyn = panel_smem_bytes((int)sizeof(T));
-    static bool attr_set = false;
-    if (!attr_set) {
-      if (cudaFuncSetAttribute((const void*)alpha_kernel<T, RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) !=
-          cudaSuccess)
-        return SA_ERR_CUDA;
-      attr_set = true;
-    }
+    // set on every launch: the attribute belongs to the current device
+    if (cudaFuncSetAttribute((const void*)alpha_kernel<T, RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) !=
+        cudaSuccess)
+      return SA_ERR_CUDA;
   } else {
     A.panel = PanelArgs{};
   }

@@ -377,27 +377,21 @@ double panel_alg_bytes(const sa_handle* h) {
   return b;
 }
 
-// The standalone operator through the panel layout (sa_spmv_scaled when the panel SpMV is on).
+// The standalone operator through the panel layout (sa_spmv_scaled when the panel SpMV is on). The
+// dynamic shared-memory attribute is set on every launch: it belongs to the current device.
 int panel_spmv_launch(sa_handle* h, const void* u, const void* x, const void* sigma, double rho, void* y) {
-  static bool attr_set[2] = {false, false};
   int* err = (int*)(h->red + 20);
   PN_CUDA(cudaMemsetAsync(err, 0, sizeof(int), h->stream));
   const PanelArgs P = panel_args(h);
   const int grid = std::min(h->panel_blocks, h->sm_count);
   if (h->prec == 32) {
     auto k = panel_spmv_kernel<float, int>;
-    if (!attr_set[0]) {
-      PN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_smem_bytes(4)));
-      attr_set[0] = true;
-    }
+    PN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_smem_bytes(4)));
     k<<<grid, kThreads, panel_smem_bytes(4), h->stream>>>(P, (const float*)u, (const float*)x, (const float*)sigma,
                                                           (float)rho, (float*)y, err);
   } else {
     auto k = panel_spmv_kernel<double, int>;
-    if (!attr_set[1]) {
-      PN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_smem_bytes(8)));
-      attr_set[1] = true;
-    }
+    PN_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, panel_smem_bytes(8)));
     k<<<grid, kThreads, panel_smem_bytes(8), h->stream>>>(P, (const double*)u, (const double*)x, (const double*)sigma,
                                                           rho, (double*)y, err);
   }

@@ -144,76 +144,208 @@ def spmv_bytes(n, nnz, rp_bytes, t):
     return nnz * (4 + t) + (n + 1) * rp_bytes + 3 * n * t
 
 
+def workload_name(args):
+    """The workload string both arms print."""
+    return (f"BA(n=2^{args.log2n}, m={args.m}) J=-A, {args.num_alphas} alphas sqrt schedule, diagonal predictor, "
+            f"eigsh_tol 1e-6, batched local search")
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def blas_threads():
+    """BLAS / OpenMP thread pools of this process (threadpoolctl), for the CPU baseline's record."""
+    try:
+        from threadpoolctl import threadpool_info
+        return [{"api": d.get("user_api"), "lib": d.get("internal_api"), "threads": d.get("num_threads")}
+                for d in threadpool_info()]
+    except Exception as e:      # threadpoolctl missing: say so
+        return [{"error": str(e)}]
+
+
+def oracle_graph(args):
+    """(n, rowptr int64, col int32, val float32) of the benchmark graph, written by the oracle's
+    stand-alone executable (oracle/_bin/ba_graph, built from the same generator source), so that the
+    CPU reference process loads none of the product's libraries."""
+    import tempfile
+    from oracle import build_tools
+    exe = build_tools.BIN if build_tools.BIN.exists() else build_tools.build()
+    n = 1 << args.log2n
+    with tempfile.TemporaryDirectory() as tmp:
+        path = Path(tmp) / "graph.bin"
+        subprocess.run([str(exe), "ba", str(n), str(args.m), "42", "0", str(path)], check=True)
+        raw = np.fromfile(path, dtype=np.uint8)
+    n_, nnz = np.frombuffer(raw[:16], dtype=np.int64)
+    o = 16
+    rowptr = np.frombuffer(raw[o:o + 8 * (n_ + 1)], dtype=np.int64)
+    o += 8 * (int(n_) + 1)
+    col = np.frombuffer(raw[o:o + 4 * nnz], dtype=np.int32)
+    o += 4 * int(nnz)
+    val = np.frombuffer(raw[o:o + 4 * nnz], dtype=np.float32)
+    return int(n_), rowptr, col, val
+
+
+class CpuSweep:
+    """The oracle's sweep of the benchmark workload (SciPy ARPACK eigsh + NumPy local search on
+    `threads` host threads), advanced alpha by alpha in schedule order with the reference's warm-start
+    chain (models/spectral_annealing.py:568-669): only alpha 0 starts cold. `timed_alpha(t)` solves
+    alpha t - 1 untimed (warm-started from wherever the chain is) and then times alpha t, warm-started
+    from its true predecessor, as in a full sweep."""
+
+    def __init__(self, J, num_alphas, threads, seed=42):
+        from oracle import specann_oracle as O
+        self.O = O
+        self.J = J
+        self.pre = O.prelude(J, 32, threads=threads)
+        self.alphas = O.alpha_schedule("sqrt", num_alphas)
+        self.rng = np.random.default_rng(seed)
+        self.threads = threads
+        self.pos = -1
+        self.y_last = self.y_prev = self.lam = self.a_prev = None
+        self.spins = []
+
+    def _advance(self, i):
+        res = self.O.solve_alpha(self.pre, self.alphas[i], i, self.a_prev, self.y_last, self.y_prev, self.lam,
+                                 rng=self.rng)
+        self.y_prev, self.y_last = self.y_last, res.y
+        self.lam, self.a_prev, self.pos = res.lambda1, self.alphas[i], i
+        return res
+
+    def timed_alpha(self, t):
+        if self.pos < t - 1:
+            self._advance(t - 1)
+        t0 = time.perf_counter()
+        res = self._advance(t)
+        dt = time.perf_counter() - t0
+        self.spins.append(self.O.round_spins(res.x))
+        return dt
+
+    def timed_ls_pass(self, k, seed):
+        """Seconds per local-search pass over k candidates: two main-loop passes over k candidates (the
+        rounded spins of the timed alphas, padded with seeded perturbations of them) divided by 3 (the
+        initial field product costs about one pass), a slight underestimate of a pass."""
+        base = self.spins[-1] if self.spins else np.ones(self.J.shape[0], dtype=np.int8)
+        rng = np.random.default_rng(seed)
+        S = [s for s in self.spins[-k:]]
+        while len(S) < k:
+            flip = rng.random(base.size) < 0.05
+            S.append(np.where(flip, -base, base).astype(np.int8))
+        t0 = time.perf_counter()
+        self.O.local_search(self.J, np.stack(S), seed=seed, max_iterations=2, num_rounds=0, threads=self.threads)
+        return (time.perf_counter() - t0) / 3.0
+
+
+def spread_targets(count, num_alphas):
+    """`count` alpha indices spread evenly over 1 .. num_alphas - 1 (alpha 0, the cold start, excluded)."""
+    if count <= 1:
+        return [num_alphas // 2]
+    return [1 + int(round(s * (num_alphas - 2) / (count - 1))) for s in range(count)]
+
+
+def cpu_solve_estimate(sweep, t_alpha, t_pass, k_ls, args):
+    """One full solve from one timed alpha and one timed local-search pass: num_alphas x the alpha's
+    time + (candidates x passes of a full solve) x the per-candidate pass time."""
+    return t_alpha * args.num_alphas + t_pass / k_ls * args.ref_candidates * args.ref_ls_passes
+
+
 def run_reference(args, rank, world):
-    """CPU reference pipeline (the oracle port: SciPy ARPACK eigsh + NumPy local search; the
-    reference's own path is CuPy-only and cannot run on a host) on a bounded sample per step,
-    extrapolated to one full solve: `cpu_sample_alphas` consecutive warm-started alphas (the start
-    rotates with the step) x num_alphas / sample, plus 4 local-search passes over their candidates
-    scaled to `ref_candidates` candidates x `ref_ls_passes` passes (the candidates and passes a full
-    solve of this workload runs; the GPU local search is bit-exact with this one, so its counts
-    apply)."""
+    """The reference arm: the CPU reference pipeline (the oracle port; the reference's own path is
+    CuPy-only) on the same workload, one alpha of the sweep per step, spread over the schedule. Each
+    step times one alpha warm-started from its true predecessor plus one local-search pass, and is
+    extrapolated to a full solve (cpu_solve_estimate); `value` is the mean over the timed steps. Under
+    torchrun only rank 0 runs."""
     if rank != 0:
         return
     import scipy.sparse as sp
-    from oracle import specann_oracle as O
-    n, rowptr, col, val = make_graph(args)
-    J = sp.csr_matrix((val.astype(np.float64), col, rowptr.astype(np.int32 if rowptr[-1] < 2**31 else np.int64)),
-                      shape=(n, n))
-    k = args.cpu_sample_alphas
-    times = []
-    for step in range(args.warmup + args.steps):
-        start_idx = (step * k) % args.num_alphas
-        t0 = time.perf_counter()
-        out = O.solve(J, precision=args.precision, num_alphas=args.num_alphas, seed=42 + step,
-                      alpha_subset=list(range(start_idx, min(args.num_alphas, start_idx + k))), use_local_search=False)
-        t_eig = time.perf_counter() - t0
-        S = np.stack(out.candidates) if out.candidates else np.ones((1, n), dtype=np.int8)
-        t0 = time.perf_counter()
-        O.local_search(J, S, seed=42 + step, max_iterations=4, num_rounds=0)
-        t_ls = time.perf_counter() - t0
-        dt = t_eig * args.num_alphas / k + t_ls / 4 / S.shape[0] * args.ref_ls_passes * args.ref_candidates
+    n, rowptr, col, val = oracle_graph(args)
+    J = sp.csr_matrix((val.astype(np.float64), col, rowptr), shape=(n, n))
+    threads = host_threads()
+    sweep = CpuSweep(J, args.num_alphas, threads)
+    targets = spread_targets(args.warmup + args.steps, args.num_alphas)
+    k_ls = 16
+    est, t_alphas, t_passes = [], [], []
+    for step, t in enumerate(targets):
+        ta = sweep.timed_alpha(t)
+        tp = sweep.timed_ls_pass(k_ls, seed=42 + step)
         if step >= args.warmup:
-            times.append(dt)
-    value = float(np.mean(times))
-    sample = (f"{k} consecutive warm-started alphas of {args.num_alphas} per step (x{args.num_alphas / k:g}) + 4 "
-              f"local-search passes over their candidates, scaled to {args.ref_candidates} candidates x "
-              f"{args.ref_ls_passes} passes; SciPy ARPACK eigsh and NumPy (single-threaded)")
+            est.append(cpu_solve_estimate(sweep, ta, tp, k_ls, args))
+            t_alphas.append(ta)
+            t_passes.append(tp)
+    value = float(np.mean(est))
+    timed = targets[args.warmup:]
+    sample = (f"per step one alpha of the {args.num_alphas}-alpha sqrt sweep (indices {timed[0]}..{timed[-1]}, "
+              f"spread evenly; each warm-started from its true predecessor, solved untimed just before) x "
+              f"{args.num_alphas}, mean {np.mean(t_alphas):.3f} s/alpha; plus one local-search pass over {k_ls} "
+              f"candidates ({np.mean(t_passes):.3f} s) scaled to {args.ref_candidates} candidates x "
+              f"{args.ref_ls_passes} passes (the GPU solve's counts; its local search is bit-exact with this one); "
+              f"SciPy ARPACK eigsh + NumPy, sparse products on {threads} threads")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value * 1000.0, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == 32 else "f64",
-            "data": "synthetic (seeded BA generator)", "impl": "reference",
-            "config": {"workload": f"BA(n=2^{args.log2n}, m={args.m}) J=-A, {args.num_alphas} alphas sqrt schedule",
-                       "n": n, "nnz": int(rowptr[-1])},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+            "data": "synthetic (seeded BA generator, J = -A)", "impl": "reference",
+            "config": {"workload": workload_name(args), "n": n, "nnz": int(rowptr[-1])},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                             "host_cpu_count": os.cpu_count(), "blas": blas_threads(),
+                             "extrapolation": f"x{args.num_alphas} per alpha; local search x"
+                                              f"{args.ref_candidates * args.ref_ls_passes / k_ls:g} per pass"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
-def cpu_baseline_sample(args, n, rowptr, col, val, k_gpu, passes_gpu, ls_sample_passes=4):
-    """The oracle pipeline (SciPy ARPACK eigsh + NumPy local search, one core) on a bounded sample,
-    extrapolated to one full solve: the first `cpu_sample_alphas` warm-started alphas (x num_alphas /
-    sample), plus `ls_sample_passes` local-search passes over their candidates, scaled to the
-    candidates and passes the GPU solve of the same workload used (k_gpu, passes_gpu)."""
-    import scipy.sparse as sp
+def cpu_baseline_sample(args, J, k_gpu, passes_gpu, count=4):
+    """The ours arm's CPU baseline: the oracle sweep on a bounded sample (`count` alphas spread over the
+    schedule, each warm-started from its true predecessor, plus one local-search pass each), extrapolated
+    to one full solve with the GPU solve's candidate and pass counts."""
+    threads = host_threads()
+    sweep = CpuSweep(J, args.num_alphas, threads)
+    k_ls = 16
+    targets = spread_targets(count, args.num_alphas)
+    ta, tp = [], []
+    t_all = time.perf_counter()
+    for i, t in enumerate(targets):
+        ta.append(sweep.timed_alpha(t))
+        tp.append(sweep.timed_ls_pass(k_ls, seed=42 + i))
+    wall = time.perf_counter() - t_all
+    value = float(np.mean(ta)) * args.num_alphas + float(np.mean(tp)) / k_ls * k_gpu * passes_gpu
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{count} alphas of the {args.num_alphas}-alpha sqrt sweep (indices {targets}), each "
+                      f"warm-started from its true predecessor (solved untimed), mean {np.mean(ta):.3f} s/alpha "
+                      f"x{args.num_alphas}; one local-search pass over {k_ls} candidates per alpha "
+                      f"({np.mean(tp):.3f} s) scaled to the GPU solve's {k_gpu} candidates x {passes_gpu} passes; "
+                      f"SciPy ARPACK eigsh + NumPy, sparse products on {threads} threads ({wall:.0f} s of CPU work)",
+            "host_cpu_count": os.cpu_count(), "blas": blas_threads()}
+
+
+def full_solve_baselines(args):
+    """Whole 128-alpha solves of the two small configurations on both sides: C1 (ER(1024, 20/1023),
+    linear schedule) and C2 (BA(2^16, 20), sqrt schedule), local search on, seed 42. The CPU side is
+    the oracle pipeline on all host threads; the GPU side is SpectralAnnealing.solve on the host CSR
+    (its uploads inside the time)."""
+    import torch
     from oracle import specann_oracle as O
-    J = sp.csr_matrix((val.astype(np.float64), col, rowptr.astype(np.int32 if rowptr[-1] < 2**31 else np.int64)),
-                      shape=(n, n))
-    k = args.cpu_sample_alphas
-    t0 = time.perf_counter()
-    out = O.solve(J, precision=args.precision, num_alphas=args.num_alphas, seed=42, alpha_subset=list(range(k)),
-                  use_local_search=False)
-    t_eig = time.perf_counter() - t0
-    S = np.stack(out.candidates) if out.candidates else np.ones((1, n), dtype=np.int8)
-    t0 = time.perf_counter()
-    O.local_search(J, S, seed=42, max_iterations=ls_sample_passes, num_rounds=0)
-    t_ls = time.perf_counter() - t0
-    per_pass_per_cand = t_ls / ls_sample_passes / S.shape[0]
-    value = t_eig * args.num_alphas / k + per_pass_per_cand * passes_gpu * k_gpu
-    return {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{k} warm-started alphas of {args.num_alphas} ({t_eig:.1f} s, x{args.num_alphas / k:g}) + "
-                      f"{ls_sample_passes} local-search passes over {S.shape[0]} candidates ({t_ls:.1f} s), scaled to "
-                      f"the GPU solve's {k_gpu} candidates x {passes_gpu} passes; SciPy ARPACK eigsh and NumPy, "
-                      f"single-threaded"}
+    from specann_b200 import graphs
+    from specann_b200.spectral_annealing import SpectralAnnealing
+    threads = host_threads()
+    cases = {"C1 ER(1024, p=20/1023) linear x128": (graphs.erdos_renyi(1024, 20 / 1023, seed=42), "linear"),
+             "C2 BA(2^16, m=20) sqrt x128": (graphs.barabasi_albert(1 << 16, 20, seed=42), "sqrt")}
+    out = {}
+    for name, (J, sched) in cases.items():
+        SpectralAnnealing("w.txt", "w", random_seed=42, schedule=sched, num_alphas=4, write_results=False).solve(J)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e_gpu, _, _ = SpectralAnnealing("f.txt", "f", random_seed=42, schedule=sched, write_results=False).solve(J)
+        torch.cuda.synchronize()
+        t_gpu = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        res = O.solve(J, seed=42, schedule=sched, num_alphas=args.num_alphas, threads=threads)
+        t_cpu = time.perf_counter() - t0
+        out[name] = {"gpu_s": t_gpu, "cpu_s": t_cpu, "cpu_cores": threads, "gpu_best_energy": e_gpu,
+                     "cpu_best_energy": res.best_energy}
+    return out
 
 
 def run_batch(args, rank, world, local):
@@ -498,10 +630,6 @@ def main():
         torch.cuda.synchronize()
         ms_ = s0.elapsed_time(s1) / args.spmv_reps
         sb_ = spmv_bytes(n, nnz, rp_np.itemsize, t)
-        if layout == "panel":
-            sb_ = eng.panel_info()["matrix_bytes"] + 3 * n * t
-        elif layout == "split":
-            sb_ = eng.split_bytes() + 3 * n * t
         hbm_, kind_ = peaks()
         print(json.dumps({"spmv_only": True, "layout": layout, "n": n, "nnz": nnz, "ms": ms_, "bytes": sb_,
                           "GBps": sb_ / ms_ / 1e6, "frac": sb_ / ms_ / 1e6 / hbm_, "peak_source": kind_}))
@@ -560,14 +688,16 @@ def main():
     eng = Engine(n, nnz, precision=args.precision, ncv_max=33, max_candidates=1)
     eng.bind(d_rowptr, d_col, d_val)
     layout = getattr(s, "operator_layout", "worklist")
+    # algorithmic bytes of one application (the CSR formula: nnz (col + value) + row pointers + x, s,
+    # y); the layout's own stream (packed panel words, split partial sums) is reported beside it
     sb = spmv_bytes(n, nnz, rp_np.itemsize, t)
+    stream_b = sb
     if layout == "panel":
-        # the solve's operator layout: the matrix stream of the panel layout + x, s, y
         eng.build_panels()
-        sb = eng.panel_info()["matrix_bytes"] + 3 * n * t
+        stream_b = eng.panel_info()["matrix_bytes"] + 3 * n * t
     elif layout == "split":
         eng.build_splits()
-        sb = eng.split_bytes() + 3 * n * t
+        stream_b = eng.split_bytes() + 3 * n * t
     x = torch.randn(n, device=dev, dtype=torch.float32 if args.precision == 32 else torch.float64)
     y = torch.empty_like(x)
     for _ in range(3):
@@ -604,8 +734,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if args.precision == 32 else "f64",
         "data": "synthetic (seeded BA generator, J = -A)",
-        "config": {"workload": f"BA(n=2^{args.log2n}, m={args.m}) J=-A, {args.num_alphas} alphas sqrt schedule, "
-                               f"diagonal predictor, eigsh_tol 1e-6, batched local search",
+        "config": {"workload": workload_name(args),
                    "n": n, "nnz": nnz, "precision": args.precision, "replicas": world,
                    "l2": "inputs larger than L2 (CSR %.0f MB > 126 MB)" % ((rp_np.nbytes + col.nbytes + nnz * t) / 1e6),
                    "best_energy": float(energies[-1]) if energies else None},
@@ -622,17 +751,20 @@ def main():
                      "peak_source": peak_kind,
                      "alpha_kernel_ms_per_solve": st["alpha_ms"], "alpha_launches_per_solve": st["alpha_launches"],
                      "spmvs_per_solve": st["spmvs"], "ls_kernel_ms_per_solve": st["ls_ms"],
+                     "ls_phase_ms": dict(zip(("setup", "decide", "scatter", "final"),
+                                            [round(x, 3) for x in st.get("ls_phase_ms", [0.0] * 4)])),
                      "alpha_phase_ms": dict(zip(("setup", "spmv", "dots", "update_ritz", "restart", "final"),
                                                [round(x, 3) for x in st.get("phase_ms", [0.0] * 6)])),
                      "lanczos_iterations": lanczos},
         "spmv": {"achieved": spmv_gbs, "peak": hbm, "unit": "GB/s", "frac": spmv_gbs / hbm,
-                 "ms": spmv_ms, "bytes": sb, "layout": layout},
+                 "ms": spmv_ms, "bytes": sb, "layout": layout, "layout_stream_bytes": stream_b},
         "clocks": clk,
         "gpu_launches": int(launches),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(args, n, rowptr, col, val, int(s._num_candidates or 1),
+        line["cpu_baseline"] = cpu_baseline_sample(args, J_host, int(s._num_candidates or 1),
                                                    int(getattr(s, "_ls_passes", 1)))
+        line["cpu_baseline"]["full_solves"] = full_solve_baselines(args)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

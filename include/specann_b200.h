@@ -106,6 +106,9 @@ typedef struct {
   int32_t final_passes;         /* passes run by the final sweep */
   int32_t integer_gains;        /* 1: int32 gains (bit-exact); 0: FP64 gains */
   int64_t total_flips;
+  double phase_ms[4];           /* device time by phase: set-up (fields, energies), decide (passes'
+                                   selection, decisions and blocking check), scatter (field updates and
+                                   the stopping rules), final (energies after, refined spins) */
 } sa_ls_result;
 
 /* ---- workspace and handle ------------------------------------------------------------------ */
@@ -133,6 +136,15 @@ int sa_set_matrix(sa_handle* h, const void* rowptr, const int32_t* col, const vo
  * fused operator of NAlphaOperator/SRhoOperator (models/spectral_annealing.py:29-53). x, y are
  * device vectors of the handle's precision. */
 int sa_spmv_scaled(sa_handle* h, double alpha, double rho, const void* x, void* y);
+
+/* Status of the asynchronous standalone operator since the last query: sa_spmv_scaled on the
+ * column-panel layout waits (bounded) for each staged panel, and a wait that runs out leaves y
+ * partly written and records SA_ERR_BARRIER_TIMEOUT in a sticky word of the handle. This call
+ * synchronises the handle's stream, returns that word in *status (SA_OK when every application since
+ * the last query completed) and clears it. The work-list and split layouts have no waits and always
+ * report SA_OK. No reference counterpart (CuPy's SpMV, models/spectral_annealing.py:38-41, has no
+ * device-side waits). */
+int sa_operator_status(sa_handle* h, int32_t* status);
 
 /* SpMV stream policy (every kernel that applies the operator). packed_columns = 1 (the default):
  * when every coupling of the bound matrix has the same magnitude w, the work-list SpMV streams one
@@ -219,6 +231,53 @@ int sa_local_search(sa_handle* h, const sa_ls_params* p, void* ls_workspace, siz
 /* Energies E = -1/2 s^T J s of candidate slots 0..k-1 (no local search): _batch_energies /
  * fp32_energies, models/spectral_annealing.py:693-707, :962-976. */
 int sa_energies(sa_handle* h, int32_t k, void* ls_workspace, size_t ls_bytes, double* energies);
+
+/* ---- guarded local-search policies (ls_policy other than "default") ------------------------------
+ * The refiners of models/local_search_guards/ (policies.py:13-69, registry.py:8-13) over candidate
+ * slots first_slot .. first_slot + k - 1; refined spins go to the refined store. Node selection uses
+ * the same counter-based stream as sa_local_search; decisions use exact integer gains for integer
+ * couplings. */
+typedef enum {
+  SA_GUARD_FIXED = 1,            /* Fixed Guard: safe_flip_refinement, models/spectral_annealing_safe.py:1035-1335,
+                                    models/local_search_guards/safe_fixed.py */
+  SA_GUARD_ADAPTIVE = 2,         /* Adaptive Guard: the same with per-candidate batch adaptation,
+                                    models/local_search_guards/safe_adaptive.py, models/safe_update_policy.py:68-95 */
+  SA_GUARD_INDEPENDENT_SET = 3,  /* Independent-Set: one colour class per update, models/local_search_guards/
+                                    conflict_free.py:80-367 (colouring and class order from the host) */
+  SA_GUARD_SEQUENTIAL = 4        /* Sequential-Oracle: exact one-flip steepest descent,
+                                    models/local_search_guards/sequential_oracle.py:26-219 */
+} sa_guard_policy;
+
+typedef struct {
+  int32_t k;                     /* candidates */
+  int32_t first_slot;
+  int32_t policy;                /* sa_guard_policy */
+  int32_t max_iterations;        /* main-phase rounds (max_local_iterations) */
+  double subset_fraction;        /* 0.9 */
+  double final_sweep_fraction;   /* 1.0 */
+  int32_t final_sweep_iters;     /* 25 */
+  int32_t num_rounds;            /* 25 */
+  uint64_t seed;                 /* node-selection stream seed */
+  const int32_t* colors;         /* SA_GUARD_INDEPENDENT_SET: device colour of every node */
+  const int32_t* color_seq;      /* SA_GUARD_INDEPENDENT_SET: device colour class of every update
+                                    (max_iterations + final_sweep_iters * num_rounds entries) */
+  int32_t num_colors;
+  int32_t reserved;
+} sa_guard_params;
+
+typedef struct {
+  int32_t status;                /* SA_OK; SA_ERR_NOT_CONVERGED when the oracle stopped at 100 n steps */
+  int32_t rounds;                /* main-phase rounds (guards), updates (independent set) or steps (oracle):
+                                    the iteration count the reference reports */
+  int32_t final_rounds;          /* final-phase rounds (guards) */
+  int32_t accepted, rejected;    /* guarded candidate updates accepted / rejected */
+  int32_t integer_gains;         /* 1: exact integer arithmetic */
+  int64_t flips;                 /* applied (node, chunk) updates; oracle: flips */
+} sa_guard_result;
+
+int sa_guard_workspace_size(sa_handle* h, int32_t k, size_t* bytes);
+int sa_guard_search(sa_handle* h, const sa_guard_params* p, void* workspace, size_t bytes,
+                    double* energies_before, double* energies_after, sa_guard_result* result);
 
 /* ---- differentiation form: adjoint of the leading eigenvector ------------------------------------
  * No counterpart in the reference (it has no gradients). With per-vertex exponents a (a_i = alpha +
@@ -366,10 +425,22 @@ int sa_batch_destroy(sa_batch* b);
  * array inside the library (8 MiB per GPU, held until the process exits), so it allocates nothing.
  * n > SA_NOALLOC_MAX_N is rejected with SA_ERR_INVALID_ARG. The first call on each device looks up
  * the array's device address; make that first call before any stream capture. All calls share the
- * array: calls that overlap on the GPU race, so serialise them. */
+ * array: calls that overlap on the GPU race, so serialise them. The row pointers must be a valid CSR
+ * of nnz entries; a column outside [0, n) is skipped (its product counts as zero), and a matrix
+ * whose couplings are all zero gives y = rho x. */
 int sa_spmv_scaled_noalloc(int64_t n, int64_t nnz, const int32_t* rowptr, const int32_t* col,
                            const float* val, double alpha, double rho, const float* x, float* y,
                            void* stream);
+
+/* Diagnostics of the bounded grid barrier that separates the phases of the persistent kernels (no
+ * reference counterpart): one launch of `blocks` CTAs (1 .. the SM count) that meet at one barrier of
+ * `expected` arrivals, each waiting at most spin_limit sleeps of ~64 ns (1 .. 2^25). scratch: a
+ * caller-owned device buffer of at least 16 + 4 * blocks bytes, 16-byte aligned. Synchronises
+ * `stream`. *status: the barrier's error word (SA_OK, or SA_ERR_BARRIER_TIMEOUT when a wait ran out,
+ * e.g. with expected > blocks); *passed_blocks: CTAs whose barrier returned success; *epilogues:
+ * CTAs that ran the last-arrival epilogue (1 on success, 0 when nobody arrives last). */
+int sa_barrier_selftest(int32_t blocks, int32_t expected, uint64_t spin_limit, void* scratch, size_t scratch_bytes,
+                        int32_t* status, int32_t* passed_blocks, int32_t* epilogues, void* stream);
 
 /* Version string of the library. */
 const char* sa_version(void);

@@ -53,6 +53,33 @@ class NumericalFailure(RuntimeError):
 # Prelude, schedule, operators, shift
 # ----------------------------------------------------------------------------------------------
 
+class ThreadedCSR:
+    """Row-block parallel products of a CSR matrix for the timed CPU baseline: SciPy's sparse kernels
+    release the GIL, so T row blocks multiplied on T threads use T host cores. Results equal the
+    single-threaded product (each row's sum is computed the same way). `data`, `indices`, `indptr`
+    and `shape` are those of the whole matrix."""
+
+    def __init__(self, A, threads: int):
+        from concurrent.futures import ThreadPoolExecutor
+        self.A = sp.csr_matrix(A)
+        self.shape, self.dtype = self.A.shape, self.A.dtype
+        self.data, self.indices, self.indptr = self.A.data, self.A.indices, self.A.indptr
+        n = self.A.shape[0]
+        cuts = np.searchsorted(self.A.indptr, np.linspace(0, self.A.nnz, threads + 1)).clip(0, n)
+        cuts[0], cuts[-1] = 0, n
+        self.blocks = [self.A[a:b] for a, b in zip(cuts[:-1], cuts[1:]) if b > a]
+        self.pool = ThreadPoolExecutor(max(1, len(self.blocks)))
+
+    def __matmul__(self, X):
+        parts = list(self.pool.map(lambda B: B @ X, self.blocks))
+        return np.concatenate(parts, axis=0)
+
+
+def threaded(A, threads: int):
+    """A itself for one thread, else its row-block parallel wrapper."""
+    return A if threads <= 1 else ThreadedCSR(A, threads)
+
+
 @dataclass
 class Prelude:
     J: sp.csr_matrix          # couplings in the working dtype (unscaled)
@@ -61,9 +88,10 @@ class Prelude:
     c: float                  # max degree (normalisation factor)
     d: np.ndarray             # deg / c in the working dtype
     dtype: type
+    op: object = None         # J / c for products (a row-block threaded wrapper for the CPU baseline)
 
 
-def prelude(J, precision: int = 32) -> Prelude:
+def prelude(J, precision: int = 32, threads: int = 1) -> Prelude:
     """models/spectral_annealing.py:270-288: device CSR, absolute degrees, c = max degree, J/c, d."""
     dt = np.float32 if precision == 32 else np.float64
     Jc = sp.csr_matrix(J.astype(dt), dtype=dt)
@@ -76,7 +104,7 @@ def prelude(J, precision: int = 32) -> Prelude:
     else:
         Js = Jc / c
     d = deg / c
-    return Prelude(J=Jc, Js=Js, deg=deg, c=float(c), d=d, dtype=dt)
+    return Prelude(J=Jc, Js=Js, deg=deg, c=float(c), d=d, dtype=dt, op=threaded(Js, threads))
 
 
 def alpha_schedule(schedule: str = "sqrt", num_alphas: int = 128, interval=(0.0, 1.0)) -> List[float]:
@@ -217,7 +245,7 @@ def solve_alpha(pre: Prelude, alpha, alpha_idx, alpha_prev, y_last, y_prev, lamb
     rho = compute_shift_rho(lambda1_prev, g, eps=shift_eps)
 
     def s_op(v):
-        return s_rho_matvec(pre.Js, dis, dt(rho), np.asarray(v, dtype=dt))
+        return s_rho_matvec(pre.op, dis, dt(rho), np.asarray(v, dtype=dt))
 
     pred_residual, pred_accepted = float("nan"), None
     if alpha_idx == 0 or disable_warm_start or y_last is None:
@@ -231,7 +259,7 @@ def solve_alpha(pre: Prelude, alpha, alpha_idx, alpha_prev, y_last, y_prev, lamb
             y_init = diagonal_predictor(y_last, pre.d, delta, rng)
         else:
             y_init = secant_predictor(y_last, y_prev)
-        v = n_alpha_matvec(pre.Js, dis, y_init)
+        v = n_alpha_matvec(pre.op, dis, y_init)
         lam = float(np.dot(y_init, v))
         r = float(np.linalg.norm(v - lam * y_init))
         pred_residual, pred_accepted = r, not r > pred_tol
@@ -332,7 +360,7 @@ def is_integer_matrix(J) -> bool:
 
 def local_search(J, spins_kn, seed: int, max_iterations: int = 1000, subset_fraction: float = 0.9,
                  final_sweep_fraction: float = 1.0, final_sweep_iters: int = 25,
-                 num_rounds: int = 25, semantics: str = "priority") -> LSResult:
+                 num_rounds: int = 25, semantics: str = "priority", threads: int = 1) -> LSResult:
     """Batched local search with the control flow of flip_refinement and gpu_final_sweep
     (models/spectral_annealing.py:1039-1112, :983-1036).
 
@@ -355,6 +383,7 @@ def local_search(J, spins_kn, seed: int, max_iterations: int = 1000, subset_frac
     else:
         Jw = sp.csr_matrix(J, dtype=np.float64)
         S = S.astype(np.float64)
+    Jw = threaded(Jw, threads)
     H = Jw @ S
     e_before = -(S * H).sum(axis=0)
     e_before = e_before // 2 if integer else 0.5 * e_before
@@ -434,6 +463,109 @@ def reference_kernel_pass(Js32, spins_kn, selected_nodes) -> np.ndarray:
     return counts
 
 
+def _reference_pass_all(Js32, Ji, S, order):
+    """reference_kernel_pass for all candidates at once (S: k x n int8, updated in place), also
+    comparing each decision with the exact integer gain at the same moment. Returns (flips per
+    candidate, decisions whose fp32 sign differs from the exact gain's)."""
+    k = S.shape[0]
+    flips = np.zeros(k, dtype=np.int64)
+    ties = 0
+    ip, ix = Js32.indptr, Js32.indices
+    dat = Js32.data.astype(np.float32)
+    idat = Ji.data
+    for node in order:
+        a, b = ip[node], ip[node + 1]
+        cols = ix[a:b]
+        sv = S[:, cols]
+        prod = dat[a:b][None, :] * sv.astype(np.float32)
+        lanes = np.zeros((k, 32), dtype=np.float32)
+        for e in range(b - a):                      # lane e % 32 accumulates in entry order
+            lanes[:, e % 32] += prod[:, e]
+        off = 16
+        while off > 0:                               # __shfl_down_sync 16, 8, 4, 2, 1
+            lanes[:, :off] = lanes[:, :off] + lanes[:, off:2 * off]
+            off //= 2
+        si = S[:, node].astype(np.float32)
+        delta = np.float32(2.0) * si * lanes[:, 0]
+        flip = delta < 0
+        exact = 2 * S[:, node].astype(np.int64) * (sv.astype(np.int64) @ idat[a:b])
+        ties += int(np.sum(flip != (exact < 0)))
+        S[flip, node] = -S[flip, node]
+        flips += flip
+    return flips, ties
+
+
+@dataclass
+class LSDeviation:
+    passes: int                    # main-loop passes compared
+    decisions: int                 # (selected node, candidate) decisions per pass, summed
+    schedule_differences: int      # decisions where the in-order in-place pass and the priority pass differ
+    arithmetic_differences: int    # in-order decisions whose fp32 sign differs from the exact integer gain
+    energy_reference: np.ndarray   # final energies of the in-order search (k)
+    energy_priority: np.ndarray    # final energies of the priority search (k)
+
+
+def ls_deviation(J, spins_kn, seed: int, max_passes: int = 1000, subset_fraction: float = 0.9) -> LSDeviation:
+    """How the engine's local search departs from the reference kernel's (integer couplings).
+
+    Both run the main loop of flip_refinement (models/spectral_annealing.py:1039-1100) over the same
+    node-selection stream. Per pass, from the same starting spins, the decisions of one in-order
+    in-place launch of update_spins_kernel_float32 (fp32 lane-strided sums and shuffle tree,
+    :821-869, warps in rank order) are compared with the priority pass's, and every in-order decision
+    is compared with the sign of the exact integer gain at that moment. Then each search continues on
+    its own trajectory until it stops (sticky active mask) or max_passes; their final energies are
+    returned. The final sweep is not included."""
+    pre = prelude(J, 32)
+    Ji = sp.csr_matrix((np.rint(J.data).astype(np.int64), J.indices, J.indptr), shape=J.shape)
+    S0 = np.asarray(spins_kn, dtype=np.int8)
+    k, n = S0.shape
+    m = selection.num_selected(n, subset_fraction)
+    coo = sp.csr_matrix(J).tocoo()
+    S_ref = S0.copy()
+    S_pri = S0.T.astype(np.int64).copy()            # n x k
+    H_pri = Ji @ S_pri
+    act_ref = np.ones(k, dtype=bool)
+    act_pri = np.ones(k, dtype=bool)
+    sched = arith = decisions = 0
+    passes = 0
+    for it in range(int(max_passes)):
+        if not act_ref.any() and not act_pri.any():
+            break
+        passes += 1
+        rank = selection.ranks(n, seed, it)
+        sel = rank < m
+        order = np.argsort(rank)[:m]
+        # priority decisions from the snapshot
+        dec = ((S_pri * H_pri) < 0) & sel[:, None]
+        if dec.any():
+            earlier = rank[coo.col] < rank[coo.row]
+            P = sp.csr_matrix((np.ones(int(earlier.sum())), (coo.row[earlier], coo.col[earlier])), shape=J.shape)
+            dec = dec & ~((P @ dec.astype(np.float64)) > 0)
+        # the in-order pass from the same spins, to count schedule differences
+        S_cmp = S_pri.T.astype(np.int8).copy()
+        before = S_cmp.copy()
+        _, t_cmp = _reference_pass_all(pre.Js, Ji, S_cmp, order)
+        ref_dec = (S_cmp != before).T
+        sched += int(np.sum(ref_dec != dec))
+        decisions += m * k
+        # advance both trajectories
+        if act_ref.any():
+            f, t = _reference_pass_all(pre.Js, Ji, S_ref, order)
+            arith += t
+            act_ref &= f > 0
+        if act_pri.any():
+            cnt = dec.sum(axis=0)
+            if dec.any():
+                dS = np.where(dec, -2 * S_pri, 0)
+                H_pri = H_pri + Ji @ dS
+                S_pri = np.where(dec, -S_pri, S_pri)
+            act_pri &= cnt > 0
+    e_ref = integer_energies(J, S_ref)
+    e_pri = integer_energies(J, S_pri.T)
+    return LSDeviation(passes=passes, decisions=decisions, schedule_differences=sched,
+                       arithmetic_differences=arith, energy_reference=e_ref, energy_priority=e_pri)
+
+
 # ----------------------------------------------------------------------------------------------
 # Full solver (SpectralAnnealing.solve)
 # ----------------------------------------------------------------------------------------------
@@ -452,14 +584,15 @@ class SolveResult:
 def solve(J, *, precision=32, schedule="sqrt", num_alphas=128, schedule_interval=(0.0, 1.0),
           pred_mode="diagonal", pred_tol=1e-3, shift_eps=1e-3, eigsh_tol=1e-6, eigsh_maxiter=1000,
           eigsh_ncv=None, disable_warm_start=False, use_local_search=True, max_local_iterations=1000,
-          seed=42, alpha_subset=None, ls_semantics="priority", energy_mode="exact") -> SolveResult:
-    """models/spectral_annealing.py:262-525 with SciPy eigsh and the snapshot local search.
+          seed=42, alpha_subset=None, ls_semantics="priority", energy_mode="exact", threads=1) -> SolveResult:
+    """models/spectral_annealing.py:262-525 with SciPy eigsh and the priority local search.
 
-    ``alpha_subset`` (indices into the schedule) runs only those alphas, in order, as a bounded
-    sample for CPU timing; the warm-start chain then links consecutive sampled alphas.
+    ``alpha_subset`` (indices into the schedule) runs only those alphas, in order; the warm-start
+    chain then links consecutive listed alphas. ``threads`` > 1 runs the sparse products on that
+    many host threads (row blocks; same results).
     """
     rng = np.random.default_rng(seed)
-    pre = prelude(J, precision)
+    pre = prelude(J, precision, threads=threads)
     alphas = alpha_schedule(schedule, num_alphas, schedule_interval)
     order = list(range(len(alphas))) if alpha_subset is None else list(alpha_subset)
     y_last = y_prev = None
@@ -497,7 +630,7 @@ def solve(J, *, precision=32, schedule="sqrt", num_alphas=128, schedule_interval
     ls = None
     if use_local_search and cand_list:
         ls = local_search(J, np.stack(cand_list), seed=seed, max_iterations=max_local_iterations,
-                          semantics=ls_semantics)
+                          semantics=ls_semantics, threads=threads)
         for rec in records:
             c = rec["candidate"]
             orig = rec["raw_energy"]

@@ -58,11 +58,27 @@ class LsParams(C.Structure):
 
 class LsResult(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("final_passes", C.c_int32),
-                ("integer_gains", C.c_int32), ("total_flips", C.c_int64)]
+                ("integer_gains", C.c_int32), ("total_flips", C.c_int64), ("phase_ms", C.c_double * 4)]
 
 
 # name -> (restype, argtypes): every symbol include/specann_b200.h declares
 SA_ADJ_GRADIENT, SA_ADJ_TANGENT, SA_ADJ_SOLVE = range(3)
+
+
+SA_GUARD_FIXED, SA_GUARD_ADAPTIVE, SA_GUARD_INDEPENDENT_SET, SA_GUARD_SEQUENTIAL = 1, 2, 3, 4
+
+
+class GuardParams(C.Structure):
+    _fields_ = [("k", C.c_int32), ("first_slot", C.c_int32), ("policy", C.c_int32), ("max_iterations", C.c_int32),
+                ("subset_fraction", C.c_double), ("final_sweep_fraction", C.c_double),
+                ("final_sweep_iters", C.c_int32), ("num_rounds", C.c_int32), ("seed", C.c_uint64),
+                ("colors", C.c_void_p), ("color_seq", C.c_void_p), ("num_colors", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class GuardResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("rounds", C.c_int32), ("final_rounds", C.c_int32), ("accepted", C.c_int32),
+                ("rejected", C.c_int32), ("integer_gains", C.c_int32), ("flips", C.c_int64)]
 
 
 class AdjointParams(C.Structure):
@@ -119,6 +135,9 @@ SIGNATURES = {
                                 C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "sa_spmv_scaled": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
     "sa_set_spmv_policy": (C.c_int, [C.c_void_p, C.c_int32]),
+    "sa_operator_status": (C.c_int, [C.c_void_p, _I32P]),
+    "sa_barrier_selftest": (C.c_int, [C.c_int32, C.c_int32, C.c_uint64, C.c_void_p, C.c_size_t, _I32P, _I32P,
+                                      _I32P, C.c_void_p]),
     "sa_panel_workspace_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_int32)]),
     "sa_panel_build": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "sa_panel_enable": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -143,6 +162,9 @@ SIGNATURES = {
     "sa_local_search": (C.c_int, [C.c_void_p, C.POINTER(LsParams), C.c_void_p, C.c_size_t,
                                   C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(LsResult)]),
     "sa_energies": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_size_t, C.POINTER(C.c_double)]),
+    "sa_guard_workspace_size": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_size_t)]),
+    "sa_guard_search": (C.c_int, [C.c_void_p, C.POINTER(GuardParams), C.c_void_p, C.c_size_t, C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double), C.POINTER(GuardResult)]),
     "sa_set_exponent_offsets": (C.c_int, [C.c_void_p, C.c_void_p]),
     "sa_adjoint_workspace_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "sa_adjoint": (C.c_int, [C.c_void_p, C.POINTER(AdjointParams), C.c_void_p, C.c_size_t,
@@ -169,6 +191,7 @@ GRAPH_SIGNATURES = {
     "sa_instance_load": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
                                    C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "sa_instance_fetch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sa_greedy_coloring": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
 }
 
 _lib = None

@@ -19,7 +19,8 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 CUDA_LIB = "libspecann_b200.so"
 GRAPH_LIB = "libspecann_graphs.so"
-CU_SOURCES = ["capi.cu", "alpha.cu", "ls.cu", "batch.cu", "adjoint.cu", "noalloc.cu", "panel.cu", "split.cu"]
+CU_SOURCES = ["capi.cu", "alpha.cu", "ls.cu", "batch.cu", "adjoint.cu", "noalloc.cu", "panel.cu", "split.cu",
+              "guard.cu"]
 HEADERS = ["common.cuh", "handle.cuh", "spmv.cuh", "policy.cuh", "alpha_body.cuh", "ls_body.cuh", "panel.cuh"]
 
 
@@ -72,7 +73,7 @@ def build_cuda(verbose: bool = False, force: bool = False) -> Path:
 def build_graphs(force: bool = False) -> Path:
     """Host library: seeded graph generators and the native instance loader."""
     out = PKG / GRAPH_LIB
-    srcs = [CSRC / "graphgen.cpp", CSRC / "loader.cpp"]
+    srcs = [CSRC / "graphgen.cpp", CSRC / "loader.cpp", CSRC / "coloring.cpp"]
     if not force and not _stale(out, srcs):
         return out
     cxx = shutil.which("g++") or "g++"

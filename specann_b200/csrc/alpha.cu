@@ -52,12 +52,14 @@ static int launch_alpha(sa_handle* h, const sa_alpha_params* p) {
   A.sqrt_c = std::sqrt(h->c);
   A.group = h->group;
   A.dense = h->dense;
+  // Algorithmic bytes of one operator application, whatever the layout: the CSR (column + value per
+  // entry, row pointers) and the vectors x, sigma, y. The panel and split layouts stream their own
+  // (smaller or larger) encodings; the roofline is stated against this figure.
   A.spmv_bytes = (double)h->nnz * (4.0 + sizeof(T)) + (double)(h->n + 1) * sizeof(RP) + 3.0 * (double)h->n * sizeof(T);
   A.use_panel = h->panel_on ? 1 : 0;
   int dyn = 0;
   if (A.use_panel) {
     A.panel = panel_args(h);
-    A.spmv_bytes = panel_alg_bytes(h) + 3.0 * (double)h->n * sizeof(T);
     dyn = panel_smem_bytes((int)sizeof(T));
     // set on every launch: the attribute belongs to the current device
     if (cudaFuncSetAttribute((const void*)alpha_kernel<T, RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) !=
@@ -72,7 +74,6 @@ static int launch_alpha(sa_handle* h, const sa_alpha_params* p) {
     A.n_splits = h->n_splits;
     for (int q = 0; q < h->n_splits; ++q) A.split[q] = split_args<T, RP>(h, q);
     A.split_part = (T*)h->split_part;
-    A.spmv_bytes = h->split_bytes + 3.0 * (double)h->n * sizeof(T);
   }
   void* args[] = {&A};
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)alpha_kernel<T, RP>, dim3(h->blocks),

@@ -424,12 +424,6 @@ __device__ void block_store_partials(const double (&v)[NV], double* part, int pw
 template <typename T>
 __device__ __forceinline__ T vload(const T* p) { return *((volatile const T*)p); }
 
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-  return t;
-}
-
 __device__ __forceinline__ unsigned long long word_mix(long long widx, unsigned int word) {
   return splitmix64(((unsigned long long)widx << 32) ^ (unsigned long long)word ^ 0xA5A5000000000000ull);
 }

@@ -222,6 +222,15 @@ __global__ void unpack_kernel(const uint32_t* bits, long long n, int8_t* out) {
     out[i] = ((bits[i >> 5] >> (i & 31)) & 1u) ? (int8_t)1 : (int8_t)-1;
 }
 
+// One bounded grid barrier of `expected` arrivals (sa_barrier_selftest): bit 0 of out[block] is the
+// barrier's result in that CTA, bit 1 is set in the CTA that ran the epilogue.
+__global__ void barrier_selftest_kernel(GridSync* gs, unsigned expected, unsigned long long spin_limit, int* out) {
+  __shared__ int s_epi;
+  if (threadIdx.x == 0) s_epi = 0;
+  const bool ok = grid_barrier_n(gs, expected, [&] { if (threadIdx.x == 0) s_epi = 1; }, spin_limit);
+  if (threadIdx.x == 0) out[blockIdx.x] = (ok ? 1 : 0) | (s_epi ? 2 : 0);
+}
+
 int grid_for(long long work, int threads, int sm_count) {
   long long b = (work + threads - 1) / threads;
   const long long cap = (long long)sm_count * 8;
@@ -370,12 +379,56 @@ int sa_create(sa_handle** out, int64_t n, int64_t nnz, int32_t rowptr64, int32_t
   if (occ < 1) { delete h; return SA_ERR_CUDA; }
   h->max_blocks = std::min(h->sm_count * occ, kMaxBlocks);
   h->blocks = h->max_blocks;
+  if (cudaMemsetAsync(h->red, 0, 8 * 64, h->stream) != cudaSuccess) { delete h; return SA_ERR_CUDA; }
   *out = h;
   return SA_OK;
 }
 
 int sa_destroy(sa_handle* h) {
   delete h;
+  return SA_OK;
+}
+
+int sa_operator_status(sa_handle* h, int32_t* status) {
+  if (!h || !status) return SA_ERR_INVALID_ARG;
+  int* word = operator_status_word(h);
+  int v = 0;
+  SA_CUDA(cudaMemcpyAsync(&v, word, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  SA_CUDA(cudaMemsetAsync(word, 0, sizeof(int), h->stream));
+  SA_CUDA(cudaStreamSynchronize(h->stream));
+  *status = v;
+  return SA_OK;
+}
+
+int sa_barrier_selftest(int32_t blocks, int32_t expected, uint64_t spin_limit, void* scratch, size_t scratch_bytes,
+                        int32_t* status, int32_t* passed_blocks, int32_t* epilogues, void* stream) {
+  int dev = 0, sms = 0;
+  SA_CUDA(cudaGetDevice(&dev));
+  SA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (blocks < 1 || blocks > sms || expected < 1 || spin_limit < 1 || spin_limit > kSpinLimit || !scratch ||
+      ((uintptr_t)scratch & 15) || scratch_bytes < sizeof(GridSync) + 4 * (size_t)blocks || !status ||
+      !passed_blocks || !epilogues)
+    return SA_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  GridSync* gs = (GridSync*)scratch;
+  int* out = (int*)((char*)scratch + sizeof(GridSync));
+  SA_CUDA(cudaMemsetAsync(scratch, 0, sizeof(GridSync) + 4 * (size_t)blocks, st));
+  barrier_selftest_kernel<<<blocks, 128, 0, st>>>(gs, (unsigned)expected, (unsigned long long)spin_limit, out);
+  count_launches(1);
+  SA_CUDA(cudaGetLastError());
+  GridSync g;
+  std::vector<int> flags(blocks);
+  SA_CUDA(cudaMemcpyAsync(&g, gs, sizeof(GridSync), cudaMemcpyDeviceToHost, st));
+  SA_CUDA(cudaMemcpyAsync(flags.data(), out, 4 * (size_t)blocks, cudaMemcpyDeviceToHost, st));
+  SA_CUDA(cudaStreamSynchronize(st));
+  int passed = 0, epi = 0;
+  for (int b = 0; b < blocks; ++b) {
+    passed += flags[b] & 1;
+    epi += (flags[b] >> 1) & 1;
+  }
+  *status = g.error;
+  *passed_blocks = passed;
+  *epilogues = epi;
   return SA_OK;
 }
 

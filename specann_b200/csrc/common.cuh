@@ -50,11 +50,14 @@ __device__ __forceinline__ int ld_volatile_i32(const int* p) {
 
 // Barrier of `expected` co-resident CTAs (a cooperative grid, or a team of CTAs inside one),
 // with an epilogue run by the last CTA to arrive (the whole CTA runs it, after every other CTA's
-// writes are visible) before the others are released. Waits are bounded: after kSpinLimit sleeps
-// the barrier records SA_ERR_BARRIER_TIMEOUT in gs->error and returns false; the caller must then
-// return.
+// writes are visible) before the others are released. Waits are bounded: after spin_limit sleeps
+// the barrier records SA_ERR_BARRIER_TIMEOUT in gs->error and returns false, and a waiting CTA
+// also stops as soon as another CTA has recorded an error; the caller must then return. The
+// decision is taken by thread 0 and shared through shared memory, so the whole CTA returns the
+// same value.
 template <class Epilogue>
-__device__ __forceinline__ bool grid_barrier_n(GridSync* gs, unsigned int expected, Epilogue&& epi) {
+__device__ __forceinline__ bool grid_barrier_n(GridSync* gs, unsigned int expected, Epilogue&& epi,
+                                               unsigned long long spin_limit = kSpinLimit) {
   __shared__ unsigned int s_last, s_gen;
   __shared__ int s_err;
   __syncthreads();
@@ -80,7 +83,8 @@ __device__ __forceinline__ bool grid_barrier_n(GridSync* gs, unsigned int expect
     unsigned long long spins = 0;
     while (ld_volatile_u32(&gs->gen) == s_gen) {
       __nanosleep(64);
-      if (++spins > kSpinLimit) {
+      if (ld_volatile_i32(&gs->error)) break;
+      if (++spins > spin_limit) {
         atomicExch(&gs->error, SA_ERR_BARRIER_TIMEOUT);
         break;
       }
@@ -99,6 +103,13 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, Epilogue&& epi) {
 
 __device__ __forceinline__ bool grid_barrier(GridSync* gs) {
   return grid_barrier_n(gs, gridDim.x, [] {});
+}
+
+// Device clock in ns (phase timers of the persistent kernels).
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -62,6 +62,7 @@ struct LsCtrl {
   long long total_flips;
   unsigned int active[4];   // candidates that have not yet had a pass without a flip
   long long counts[128];    // flips per candidate in the current pass
+  unsigned long long tph[4];  // ns by phase (set-up, decide, scatter, final)
 };
 
 struct Layout {
@@ -164,3 +165,9 @@ struct sa_handle {
   int max_blocks = 0;           // cooperative grid size cap for this device
   int blocks = 0;               // grid size used by the persistent kernels
 };
+
+namespace sa {
+// Sticky status word of the asynchronous standalone operator (sa_spmv_scaled on the panel layout):
+// a timed-out panel wait records SA_ERR_BARRIER_TIMEOUT here; sa_operator_status reads and clears it.
+inline int* operator_status_word(sa_handle* h) { return (int*)(h->red + 20); }
+}  // namespace sa

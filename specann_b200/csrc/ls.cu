@@ -137,6 +137,7 @@ int ls_run_impl(sa_handle* h, const sa_ls_params* p, void* ws, size_t bytes, dou
     res->final_passes = ctl.final_passes;
     res->integer_gains = integer ? 1 : 0;
     res->total_flips = ctl.total_flips;
+    for (int q = 0; q < 4; ++q) res->phase_ms[q] = (double)ctl.tph[q] * 1e-6;
   }
   return SA_OK;
 }

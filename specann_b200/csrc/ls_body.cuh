@@ -146,6 +146,16 @@ __device__ __forceinline__ void ls_body(const LsArgs<VT, RP, GT>& A, const Pol& 
   const long long gwarp = gtid >> 5, nwarps = nthreads >> 5;
   const long long n = A.n;
   const int cp = A.cp, ne = 32 / cp, slot = lane / cp, c = lane % cp;
+  // phase timer: the first CTA's thread 0 charges the time since its previous mark to a phase
+  const bool timer = pol.block() == 0 && threadIdx.x == 0;
+  unsigned long long t_mark = timer ? global_ns() : 0ull;
+  auto mark = [&](int ph) {
+    if (timer) {
+      const unsigned long long t = global_ns();
+      C->tph[ph] += t - t_mark;
+      t_mark = t;
+    }
+  };
 
   // ---- L0: candidate-major packed spins -> node-major bits; zero the fields -----------------
   if (pol.block() == 0 && threadIdx.x == 0) {
@@ -154,6 +164,7 @@ __device__ __forceinline__ void ls_body(const LsArgs<VT, RP, GT>& A, const Pol& 
     for (int q = 0; q < 4; ++q) C->active[q] = 0u;
     for (int q = 0; q < A.k; ++q) C->active[q >> 5] |= 1u << (q & 31);
     for (int q = 0; q < 128; ++q) C->counts[q] = 0;
+    for (int q = 0; q < 4; ++q) C->tph[q] = 0ull;
     const bool main_loop = A.p.max_iterations > 0;
     const bool final_sweep = A.p.num_rounds > 0 && A.p.final_sweep_iters > 0;
     C->phase = main_loop ? 0 : (final_sweep ? 1 : 2);
@@ -202,6 +213,7 @@ __device__ __forceinline__ void ls_body(const LsArgs<VT, RP, GT>& A, const Pol& 
   if (!pol.sync(&C->gs)) return;
   energy_phase(A, A.ebefore, s_acc, gwarp, nwarps);
   if (!pol.sync(&C->gs)) return;
+  mark(0);
 
   // ---- passes ------------------------------------------------------------------------------
   while (ld_volatile_i32(&C->phase) != 2) {
@@ -316,6 +328,7 @@ __device__ __forceinline__ void ls_body(const LsArgs<VT, RP, GT>& A, const Pol& 
     for (int q = threadIdx.x; q < A.k; q += blockDim.x)
       if (s_cnt[q]) atomicAdd((unsigned long long*)&C->counts[q], (unsigned long long)s_cnt[q]);
     if (!pol.sync(&C->gs)) return;
+    mark(1);
 
     // U: scatter field changes of the flipped (node, candidate) pairs
     const long long nwl = min(*((volatile long long*)&C->wl_count), A.wl_cap);
@@ -376,6 +389,7 @@ __device__ __forceinline__ void ls_body(const LsArgs<VT, RP, GT>& A, const Pol& 
             else if (C->phase == 1) { C->stream = kFinalStreamBase + C->round; C->m = A.m_final; }
           }
         })) return;
+    mark(2);
   }
 
   // ---- energies after, refined candidates back to candidate-major ---------------------------
@@ -389,6 +403,7 @@ __device__ __forceinline__ void ls_body(const LsArgs<VT, RP, GT>& A, const Pol& 
     const uint32_t word = __ballot_sync(0xffffffffu, bit);
     if (lane == 0) A.refined[cq * A.W + wd] = word;
   }
+  mark(3);
 }
 
 }  // namespace sa

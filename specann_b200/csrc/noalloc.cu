@@ -14,6 +14,10 @@
 // exits). Every call uses the same array and leaves the last call's values in it; the accumulator
 // that must start at zero is cleared at the start of each call. Calls whose executions overlap on
 // the GPU (for example on two streams, or from two host threads) race on the array: serialise them.
+//
+// Inputs it cannot reject without a synchronisation: a column outside [0, n) is skipped (its product
+// counts as zero) so that no read leaves the scaled input; a matrix whose couplings are all zero
+// (c = 0, where the normalisation J / c is undefined) gives the defined result N = 0, y = rho x.
 #include <cmath>
 #include <algorithm>
 #include <mutex>
@@ -34,19 +38,26 @@ static __device__ __align__(256) float g_noalloc_scratch[2 * kMaxN + 64];
 
 std::mutex g_setup_mutex;
 float* g_scratch_ptr[kMaxDevices] = {nullptr};
+int g_sm_count[kMaxDevices] = {0};
 
-// Device address of the scratch array on the current device, looked up once per device (the
-// host-side symbol is only a stand-in for the device array and must not be passed to a kernel).
-int scratch_for_current_device(float** out) {
+// Device address of the scratch array on the current device and that device's SM count, looked up
+// once per device (the host-side symbol is only a stand-in for the device array and must not be
+// passed to a kernel).
+int scratch_for_current_device(float** out, int* sms) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SA_ERR_CUDA;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
   if (!g_scratch_ptr[dev]) {
     void* p = nullptr;
+    int count = 0;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return SA_ERR_CUDA;
+    if (cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || count < 1)
+      return SA_ERR_CUDA;
+    g_sm_count[dev] = count;
     g_scratch_ptr[dev] = (float*)p;
   }
   *out = g_scratch_ptr[dev];
+  *sms = g_sm_count[dev];
   return SA_OK;
 }
 
@@ -66,6 +77,11 @@ __global__ void na_degrees(const int* rp, const float* val, long long n, float* 
 __global__ void na_scale(long long n, double alpha, const unsigned long long* cmax, const float* x,
                          float* sigma, float* u) {
   const double c = __longlong_as_double((long long)*cmax);
+  if (!(c > 0.0)) {   // no non-zero coupling: N = 0
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+      sigma[i] = u[i] = 0.0f;
+    return;
+  }
   const double half_log2_c = 0.5 * log2(c);
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const double d = (double)sigma[i] / c;
@@ -84,7 +100,10 @@ __global__ void na_spmv(const int* rp, const int* col, const float* val, long lo
   const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
   for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
     float acc = 0.0f;
-    for (int p = __ldg(rp + r) + lane; p < __ldg(rp + r + 1); p += 32) acc += __ldg(val + p) * __ldg(u + __ldg(col + p));
+    for (int p = __ldg(rp + r) + lane; p < __ldg(rp + r + 1); p += 32) {
+      const int j = __ldg(col + p);
+      if (j >= 0 && j < n) acc += __ldg(val + p) * __ldg(u + j);
+    }
     acc = sa::warp_sum(acc);
     if (lane == 0) y[r] = rho * x[r] - sigma[r] * acc;
   }
@@ -98,7 +117,8 @@ extern "C" int sa_spmv_scaled_noalloc(int64_t n, int64_t nnz, const int32_t* row
   if (n < 1 || n > kMaxN || nnz < 0 || nnz > INT32_MAX || !rowptr || !x || !y || (nnz > 0 && (!col || !val)))
     return SA_ERR_INVALID_ARG;
   float* scratch = nullptr;
-  const int st = scratch_for_current_device(&scratch);
+  int sms = 0;
+  const int st = scratch_for_current_device(&scratch, &sms);
   if (st != SA_OK) return st;
   float* sigma = scratch;
   float* u = scratch + kMaxN;
@@ -106,10 +126,10 @@ extern "C" int sa_spmv_scaled_noalloc(int64_t n, int64_t nnz, const int32_t* row
   cudaStream_t s = (cudaStream_t)stream;
   if (cudaMemsetAsync(cmax, 0, sizeof(unsigned long long), s) != cudaSuccess) return SA_ERR_CUDA;
   const int threads = 256;
-  const int blocks = (int)std::min<long long>((n + threads - 1) / threads, 148 * 8);
+  const int blocks = (int)std::min<long long>((n + threads - 1) / threads, (long long)sms * 8);
   na_degrees<<<blocks, threads, 0, s>>>(rowptr, val, n, sigma, cmax);
   na_scale<<<blocks, threads, 0, s>>>(n, alpha, cmax, x, sigma, u);
-  const int sblocks = (int)std::min<long long>((n * 32 + threads - 1) / threads, 148 * 16);
+  const int sblocks = (int)std::min<long long>((n * 32 + threads - 1) / threads, (long long)sms * 16);
   na_spmv<<<sblocks, threads, 0, s>>>(rowptr, col, val, n, (float)rho, x, sigma, u, y);
   sa::count_launches(3);
   return cudaGetLastError() == cudaSuccess ? SA_OK : SA_ERR_CUDA;

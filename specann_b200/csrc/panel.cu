@@ -380,8 +380,7 @@ double panel_alg_bytes(const sa_handle* h) {
 // The standalone operator through the panel layout (sa_spmv_scaled when the panel SpMV is on). The
 // dynamic shared-memory attribute is set on every launch: it belongs to the current device.
 int panel_spmv_launch(sa_handle* h, const void* u, const void* x, const void* sigma, double rho, void* y) {
-  int* err = (int*)(h->red + 20);
-  PN_CUDA(cudaMemsetAsync(err, 0, sizeof(int), h->stream));
+  int* err = operator_status_word(h);   // sticky until sa_operator_status reads it
   const PanelArgs P = panel_args(h);
   const int grid = std::min(h->panel_blocks, h->sm_count);
   if (h->prec == 32) {

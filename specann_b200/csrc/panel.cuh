@@ -227,16 +227,19 @@ __device__ __forceinline__ bool panel_spmv(const PanelArgs& P, const T* u, int b
         ne = __ldg(ch + (long long)(p + 1) * kWarps + 1);
       }
       const int buf = p % kPanelBufs;
-      unsigned long long spins = 0;
-      while (!mbar_try_wait(&bars[buf], (par >> buf) & 1u)) {
+      const unsigned par0 = par;   // the same in every thread of the CTA
+      // Bounded wait for panel p. A thread that gives up skips the panel's work and the CTA decides
+      // at the barrier that ends the panel (__syncthreads_or), so every thread returns together.
+      bool late = false;
+      for (unsigned long long spins = 0; !mbar_try_wait(&bars[buf], (par0 >> buf) & 1u);)
         if (++spins > kPanelSpinLimit) {
-          atomicExch(err, SA_ERR_BARRIER_TIMEOUT);
-          return false;
+          late = true;
+          break;
         }
-      }
+      late = __any_sync(0xffffffffu, late);   // the batch loop's shuffles need whole warps
       par ^= 1u << buf;
       const T* xs = (const T*)(smem + (size_t)buf * panel_buf_bytes(sizeof(T)));
-      for (long long e = cs;; e += kPanelBatchEntries) {
+      for (long long e = cs; !late; e += kPanelBatchEntries) {
         const bool more = e + kPanelBatchEntries < ce;
         unsigned nx[kPanelLane];
         T nv[kPanelLane] = {};
@@ -257,7 +260,20 @@ __device__ __forceinline__ bool panel_spmv(const PanelArgs& P, const T* u, int b
       }
       cs = ns;
       ce = ne;
-      __syncthreads();
+      if (__syncthreads_or(late)) {
+        // Give up: record the timeout, then wait (bounded again) for the copies this CTA still has
+        // in flight into its shared memory (panels p .. p + kPanelBufs - 1) before returning.
+        if (threadIdx.x == 0) {
+          atomicExch(err, SA_ERR_BARRIER_TIMEOUT);
+          for (int q = p; q < p + kPanelBufs && q < np; ++q) {
+            const int qb = q % kPanelBufs;
+            for (unsigned long long spins = 0; !mbar_try_wait(&bars[qb], (par0 >> qb) & 1u);)
+              if (++spins > kPanelSpinLimit) break;
+          }
+        }
+        __syncthreads();
+        return false;
+      }
       if (threadIdx.x == 0 && p + kPanelBufs < np) {
         fence_proxy_async();
         panel_issue<T>(P, u, p + kPanelBufs, smem, bars);

@@ -34,12 +34,15 @@ class Engine:
     """A solver handle: workspace, bound matrix, candidate store."""
 
     def __init__(self, n: int, nnz: int, precision: int = 32, ncv_max: int = 33, max_candidates: int = 128,
-                 device: Optional[torch.device] = None, stream: Optional[torch.cuda.Stream] = None):
+                 device: Optional[torch.device] = None, stream: Optional[torch.cuda.Stream] = None,
+                 rowptr64: Optional[bool] = None):
+        """rowptr64: 64-bit row pointers (the kernels' `long long` instantiations); None chooses them
+        only when nnz does not fit in int32."""
         _require_cuda()
         self.lib = _lib.load()
         self.n, self.nnz = int(n), int(nnz)
         self.precision = int(precision)
-        self.rowptr64 = self.nnz > np.iinfo(np.int32).max
+        self.rowptr64 = self.nnz > np.iinfo(np.int32).max if rowptr64 is None else bool(rowptr64)
         self.ncv_max = int(ncv_max)
         self.max_candidates = int(max_candidates)
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -87,6 +90,13 @@ class Engine:
 
     def bind(self, rowptr: torch.Tensor, col: torch.Tensor, val: torch.Tensor) -> MatrixInfo:
         """Bind device CSR tensors (kept alive by the engine) and run the prelude."""
+        want_rp = torch.int64 if self.rowptr64 else torch.int32
+        want_val = torch.float32 if self.precision == 32 else torch.float64
+        if rowptr.dtype != want_rp or col.dtype != torch.int32 or val.dtype != want_val:
+            raise ValueError(f"device CSR must be rowptr {want_rp}, col torch.int32, val {want_val}; got "
+                             f"{rowptr.dtype}, {col.dtype}, {val.dtype}")
+        if rowptr.numel() != self.n + 1 or col.numel() != self.nnz or val.numel() != self.nnz:
+            raise ValueError("device CSR sizes do not match the engine's n and nnz")
         self.d_rowptr, self.d_col, self.d_val = rowptr, col, val
         c = C.c_double()
         dmin = C.c_double()
@@ -105,6 +115,13 @@ class Engine:
         check("sa_spmv_scaled", self.lib.sa_spmv_scaled(self.h, float(alpha), float(rho), C.c_void_p(x.data_ptr()),
                                                         C.c_void_p(y.data_ptr())))
         return y
+
+    def operator_status(self) -> int:
+        """Status of the standalone operator applications since the last call (synchronises the
+        engine's stream; SA_ERR_BARRIER_TIMEOUT if a panel wait ran out)."""
+        st = C.c_int32(0)
+        check("sa_operator_status", self.lib.sa_operator_status(self.h, C.byref(st)))
+        return int(st.value)
 
     def set_spmv_policy(self, packed_columns: bool = True) -> None:
         """SpMV stream policy: packed signed columns for one-magnitude couplings."""
@@ -289,6 +306,35 @@ class Engine:
             e1.synchronize()
             self.stats["ls_ms"] += e0.elapsed_time(e1)
             self.stats["ls_launches"] += 1
+            ph = self.stats.setdefault("ls_phase_ms", [0.0] * 4)
+            for q in range(4):
+                ph[q] += res.phase_ms[q]
+        return np.array(eb[:]), np.array(ea[:]), res
+
+    def guard_search(self, policy: int, k: int, *, first_slot=0, max_iterations=1000, subset_fraction=0.9,
+                     final_sweep_fraction=1.0, final_sweep_iters=25, num_rounds=25, seed=0,
+                     colors: Optional[torch.Tensor] = None, color_seq: Optional[torch.Tensor] = None,
+                     num_colors: int = 0):
+        """Guarded local search of candidate slots first_slot .. first_slot + k - 1 (policy: one of
+        _lib.SA_GUARD_*). Returns (energies before, energies after, GuardResult)."""
+        nbytes = C.c_size_t(0)
+        check("sa_guard_workspace_size", self.lib.sa_guard_workspace_size(self.h, int(k), C.byref(nbytes)))
+        need = int(nbytes.value) + 256
+        if getattr(self, "guard_workspace", None) is None or self.guard_workspace.numel() < need:
+            self.guard_workspace = torch.empty(need, dtype=torch.uint8, device=self.device)
+        ptr = (self.guard_workspace.data_ptr() + 255) & ~255
+        p = _lib.GuardParams(k=int(k), first_slot=int(first_slot), policy=int(policy),
+                             max_iterations=int(max_iterations), subset_fraction=float(subset_fraction),
+                             final_sweep_fraction=float(final_sweep_fraction), final_sweep_iters=int(final_sweep_iters),
+                             num_rounds=int(num_rounds), seed=int(seed) & (2 ** 64 - 1),
+                             colors=C.c_void_p(colors.data_ptr()) if colors is not None else None,
+                             color_seq=C.c_void_p(color_seq.data_ptr()) if color_seq is not None else None,
+                             num_colors=int(num_colors))
+        eb = (C.c_double * k)()
+        ea = (C.c_double * k)()
+        res = _lib.GuardResult()
+        check("sa_guard_search", self.lib.sa_guard_search(self.h, C.byref(p), C.c_void_p(ptr), int(nbytes.value),
+                                                          eb, ea, C.byref(res)))
         return np.array(eb[:]), np.array(ea[:]), res
 
     def energies(self, k: int) -> np.ndarray:

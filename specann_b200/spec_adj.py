@@ -72,8 +72,6 @@ class _FixedAlpha:
         """Solve the instance with couplings J. Returns (energy, spins, time in seconds)."""
         from .engine import Engine
         start_time = time.time()
-        if self.ls_policy != "default" and self.use_local_search:
-            raise NotImplementedError(f"ls_policy {self.ls_policy!r} is not part of the B200 engine")
         Jc = as_csr(J)
         n = Jc.shape[0]
         self._seed = _seed_value(self.random_seed)
@@ -88,9 +86,16 @@ class _FixedAlpha:
         local_iterations = 0
         use_refined = False
         if self.use_local_search:
-            eb, ea, res = eng.local_search(1, max_iterations=self.max_local_iterations, seed=self._seed,
-                                           semantics=self.ls_semantics)
-            local_iterations = int(res.iterations)
+            if self.ls_policy == "default":
+                eb, ea, res = eng.local_search(1, max_iterations=self.max_local_iterations, seed=self._seed,
+                                               semantics=self.ls_semantics)
+                local_iterations = int(res.iterations)
+            else:
+                # models/spec_adj.py:130-133, models/spec_signed_lap.py (refine_candidates)
+                from .guards import run_policy
+                eb, ea, local_iterations, _ = run_policy(eng, self.ls_policy, 1,
+                                                         max_iterations=self.max_local_iterations,
+                                                         seed=self._seed, indptr=Jc.indptr, indices=Jc.indices)
             energy = float(eb[0])
             if ea[0] < eb[0]:
                 energy = float(ea[0])

@@ -171,6 +171,14 @@ class SpectralAnnealing:
             raise ValueError(f"spmv must be 'auto', 'panel', 'split' or 'worklist', got {self.spmv!r}")
         # local-search pass semantics: "priority" (independent flips, monotone) or "snapshot"
         self.ls_semantics = str(kwargs.pop("ls_semantics", "priority"))
+        # 64-bit row pointers for solve(J) (None: only when nnz does not fit in int32); solve_device
+        # follows the dtype of the row-pointer tensor it is given
+        rp64 = kwargs.pop("rowptr64", None)
+        self.rowptr64 = None if rp64 is None else bool(rp64)
+        # alpha indices whose eigenvector (device copy), shift and Ritz value are kept after the
+        # solve in self.kept_vectors[idx] = (y, rho, mu) (checks against an FP64 eigensolver)
+        self.keep_vectors = frozenset(int(i) for i in kwargs.pop("keep_vectors", ()))
+        self.kept_vectors = {}
         if self.ls_semantics not in ("priority", "snapshot"):
             raise ValueError(f"ls_semantics must be 'priority' or 'snapshot', got {self.ls_semantics!r}")
         self._extra_kwargs = kwargs
@@ -242,7 +250,8 @@ class SpectralAnnealing:
         self._check_runnable()
         Jc = as_csr(J)
         n = Jc.shape[0]
-        eng = self._make_engine(n, Jc.nnz)
+        self._host_csr = (Jc.indptr, Jc.indices)
+        eng = self._make_engine(n, Jc.nnz, self.rowptr64)
         data = Jc.data.astype(np.float32, copy=False) if (self.precision == 32) else Jc.data
         info = eng.upload_csr(Jc.indptr, Jc.indices, data)
         self._choose_operator(eng)
@@ -255,7 +264,8 @@ class SpectralAnnealing:
         start_time = time.time()
         self._check_runnable()
         n = int(rowptr.numel()) - 1
-        eng = self._make_engine(n, int(col.numel()))
+        self._host_csr = None
+        eng = self._make_engine(n, int(col.numel()), rowptr.dtype == torch.int64)
         info = eng.bind(rowptr, col, val)
         self._choose_operator(eng)
         return self._sweep(eng, info, None, start_time)
@@ -274,17 +284,15 @@ class SpectralAnnealing:
     def _check_runnable(self):
         if self.alpha is not None:
             raise ValueError("Alpha is not set")
-        if self.ls_policy != "default" and self.use_local_search:
-            raise NotImplementedError(f"ls_policy {self.ls_policy!r} (guarded local search) is not part of the "
-                                      f"B200 engine; use ls_policy='default'")
 
-    def _make_engine(self, n, nnz):
+    def _make_engine(self, n, nnz, rowptr64=None):
         from .engine import Engine
         self._seed = _seed_value(self.random_seed)
         eng_prec = 32 if self.fp32_spmv else 64
         self._capacity = min(128, self.num_alphas)
         self._ncv = default_ncv(n, self.eigsh_ncv)
-        eng = Engine(n, nnz, precision=eng_prec, ncv_max=max(self._ncv, 2), max_candidates=self._capacity)
+        eng = Engine(n, nnz, precision=eng_prec, ncv_max=max(self._ncv, 2), max_candidates=self._capacity,
+                     rowptr64=rowptr64)
         eng.profile = self.profile
         self.engine = eng
         return eng
@@ -305,6 +313,7 @@ class SpectralAnnealing:
         self._alpha_errors = 0
         self._last_alpha_error = None
         self._tangent = None
+        self.kept_vectors = {}
         for alpha_idx, alpha in enumerate(alpha_list):
             t_alpha = time.time()
             try:
@@ -324,6 +333,8 @@ class SpectralAnnealing:
             lambda1 = rho - rec.mu
             bound = (-0.5 * lambda1 * rec.degree_scale * info.c) if converged else float("nan")
             slot = cands.add_scratch(rec.signature)
+            if alpha_idx in self.keep_vectors:
+                self.kept_vectors[alpha_idx] = (eng.result_vector(), rho, rec.mu)
             tangent_spmvs = 0
             if self.pred_mode == "tangent" and not self.disable_warm_start:
                 # dy/dalpha at this eigenpair (the next alpha's start is y + dalpha t)
@@ -412,6 +423,19 @@ class SpectralAnnealing:
 
     def _refine(self, eng, k):
         """Local search of the distinct candidates: (energies before, energies after, passes)."""
+        if self.ls_policy != "default":
+            # guarded policies (models/spectral_annealing.py:540-547 -> local_search_guards.run_policy)
+            from .guards import run_policy
+            indptr = indices = None
+            if self.ls_policy == "independent_set":
+                indptr, indices = self._host_structure(eng)
+            eb, ea, iters, res = run_policy(eng, self.ls_policy, k, max_iterations=self.max_local_iterations,
+                                            seed=self._seed, indptr=indptr, indices=indices)
+            self._ls_passes = iters + int(res.final_rounds)
+            self._last_ls_summary = {"rounds": int(res.rounds), "final_rounds": int(res.final_rounds),
+                                     "accepted_updates": int(res.accepted), "rejected_updates": int(res.rejected),
+                                     "status": int(res.status)}
+            return eb, ea, iters
         if self.ls_batch:
             eb, ea, res = eng.local_search(k, max_iterations=self.max_local_iterations, seed=self._seed,
                                            semantics=self.ls_semantics)
@@ -426,6 +450,12 @@ class SpectralAnnealing:
             eb[c], ea[c] = b[0], a[0]
             used = max(used, int(res.iterations))
         return eb, ea, used
+
+    def _host_structure(self, eng):
+        """Host row pointers and columns of the bound matrix (the independent set's colouring)."""
+        if getattr(self, "_host_csr", None) is not None:
+            return self._host_csr
+        return eng.d_rowptr.cpu().numpy(), eng.d_col.cpu().numpy()
 
     # -- CSVs -----------------------------------------------------------------------------------------
     def _store_general_results(self, energy, alpha, beta, time_taken, local_search_iterations=0):

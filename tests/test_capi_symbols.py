@@ -54,7 +54,9 @@ def test_struct_layouts_match_c():
     assert ctypes.sizeof(_lib.AlphaParams) == 7 * 8 + 4 * 4 + 8 + 8 + 8 + 4 * 4
     assert ctypes.sizeof(_lib.AlphaRecord) == 4 * 4 + 7 * 8 + 8 + 4 * 4 + 8 + 6 * 8
     assert ctypes.sizeof(_lib.LsParams) == 4 * 3 + 4 + 2 * 8 + 2 * 4 + 8 + 2 * 4
-    assert ctypes.sizeof(_lib.LsResult) == 4 * 4 + 8
+    assert ctypes.sizeof(_lib.LsResult) == 4 * 4 + 8 + 4 * 8
+    assert ctypes.sizeof(_lib.GuardParams) == 4 * 4 + 2 * 8 + 2 * 4 + 8 + 2 * 8 + 2 * 4
+    assert ctypes.sizeof(_lib.GuardResult) == 6 * 4 + 8
 
 
 def test_graph_library():

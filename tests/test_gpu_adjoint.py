@@ -34,7 +34,7 @@ def rel(a, b):
 
 # (precision, Lanczos tolerance, MINRES tolerance, bound on the relative gradient error): the
 # adjoint is resolved to about the eigenpair's own accuracy, not below it
-@pytest.mark.parametrize("precision,tol,adj_tol,bound", [(64, 1e-10, 1e-8, 1e-6), (32, 1e-6, 1e-4, 5e-2)])
+@pytest.mark.parametrize("precision,tol,adj_tol,bound", [(64, 1e-10, 1e-8, 1e-6), (32, 1e-6, 1e-4, 2e-3)])
 @pytest.mark.parametrize("alpha", [0.3, 0.7])
 def test_gradient_matches_dense_oracle(J12, dense12, precision, tol, adj_tol, bound, alpha):
     L_ref, g_ref, lam_ref, _ = dense12[alpha]

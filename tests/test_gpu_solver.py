@@ -53,7 +53,7 @@ def test_sweep_matches_reference_run(golden_cases, name):
 
 @pytest.mark.parametrize("name", ["tiny_ba100_specann32", "er128_prev_linear32", "ba128_secant32"])
 def test_sweep_matches_oracle_pipeline(golden_cases, name):
-    """Same candidates (up to a global sign) and the same snapshot local search as the oracle
+    """Same candidates (up to a global sign) and the same priority local search as the oracle
     pipeline: the best energies are equal."""
     z = golden_cases[name]
     p = json.loads(str(z["params"]))
@@ -66,14 +66,94 @@ def test_sweep_matches_oracle_pipeline(golden_cases, name):
     assert e_gpu == out.best_energy
 
 
-@pytest.mark.parametrize("cls,name", [(Alpha0GPU, "tiny_ba100_specadj32"), (Alpha1GPU, "tiny_ba120_specsignedlap32")])
-def test_fixed_alpha_endpoints(golden_cases, cls, name):
+def _dense_leading(J, alpha):
+    deg = np.asarray(abs(J).sum(axis=1)).ravel()
+    M, _ = O.scaled_operator_f64(J, deg, deg.max(), alpha)
+    w, V = np.linalg.eigh(M.toarray())
+    return float(w[-1]), V[:, -1]
+
+
+@pytest.mark.parametrize("cls,name,alpha", [(Alpha0GPU, "tiny_ba100_specadj32", 0.0),
+                                            (Alpha1GPU, "tiny_ba120_specsignedlap32", 1.0)])
+def test_fixed_alpha_endpoints(golden_cases, cls, name, alpha):
+    """SpecAdj / SpecSignedLap: the leading eigenvalue against dense FP64 eigh, the rounding bit-exact
+    given the GPU's own eigenvector, the energy exact given the GPU's candidate (oracle local search);
+    in FP64 at a tight tolerance the candidate is the FP64 eigenvector's rounding and the energy is
+    the reference run's."""
     z = golden_cases[name]
     J = gold_J(z)
-    energy, spins, _ = cls(name + ".txt", "golden", random_seed=42).solve(J)
+    lam64, y64 = _dense_leading(J, alpha)
+    solver = cls(name + ".txt", "golden", random_seed=42)
+    energy, spins, _ = solver.solve(J)
     assert O.exact_energy(J, spins) == energy
-    ref = float(z["best_energy"])
-    assert energy <= ref + 0.05 * abs(ref)
+    eng = solver.engine
+    y = eng.result_vector().double().cpu().numpy()
+    M, _ = O.scaled_operator_f64(J, np.asarray(abs(J).sum(axis=1)).ravel(), abs(J).sum(axis=1).max(), alpha)
+    lam = float(y @ (M @ y))
+    assert abs(lam - lam64) <= 1e-5
+    assert np.linalg.norm(M @ y - lam * y) <= 1e-5
+    cand = eng.candidate_spins(0).cpu().numpy()
+    assert np.array_equal(cand, np.where(y >= 0, 1, -1).astype(np.int8))
+    ls = O.local_search(J, cand[None, :], seed=42)
+    assert energy == min(O.exact_energy(J, cand), float(ls.energies_after[0]))
+    # FP64, tol 1e-11: the vector is resolved far below its smallest entry
+    tight = cls(name + ".txt", "golden", random_seed=42, precision=64, eigsh_tol=1e-11)
+    e64, s64, _ = tight.solve(J)
+    c64 = tight.engine.candidate_spins(0).cpu().numpy()
+    ref_spins = O.round_spins(y64)
+    assert np.array_equal(c64, ref_spins) or np.array_equal(c64, -ref_spins)
+    assert e64 == float(z["best_energy"])
+
+
+@pytest.mark.parametrize("name", ["tiny_ba20_specann32", "tiny_ba100_specann32", "tiny_ba190_specann64",
+                                  "ba128_secant32", "er128_prev_linear32", "er1024_linear16_nols32"])
+def test_predictor_decisions_against_reference_rows(golden_cases, name):
+    """Each alpha of the reference run re-solved on the GPU from the reference's own warm-start chain
+    (y_last, y_prev and the previous eigenvalue): the predictor's residual and accept decision match
+    the reference's rows (a decision within 1e-5 of pred_tol may go either way, at most once), and
+    the leading eigenvalue matches."""
+    from specann_b200 import _lib
+    from specann_b200.engine import Engine
+    from specann_b200.spectral_annealing import compute_shift_rho, default_ncv, gershgorin_bound
+    z = golden_cases[name]
+    p = json.loads(str(z["params"]))
+    prec = p.get("precision", 32)
+    mode = {"diagonal": _lib.SA_START_DIAGONAL, "secant": _lib.SA_START_SECANT,
+            "prev": _lib.SA_START_PREV}[p.get("pred_mode", "diagonal")]
+    J = gold_J(z)
+    n = J.shape[0]
+    eng = Engine(n, J.nnz, precision=prec, ncv_max=default_ncv(n, None), max_candidates=1)
+    info = eng.upload_csr(J.indptr, J.indices, J.data.astype(np.float32 if prec == 32 else np.float64))
+    dt = torch.float32 if prec == 32 else torch.float64
+    ys = z["cap_y"]
+    alphas = z["cap_alpha"]
+    borderline = 0
+    for a in range(1, len(alphas)):
+        # chain: y_prev = reference y[a-2], y_last = reference y[a-1]
+        if a >= 2:
+            eng.set_last_vector(torch.tensor(ys[a - 2], dtype=dt, device="cuda"))
+            eng.round_vector(float(alphas[a - 1]), torch.tensor(ys[a - 1], dtype=dt, device="cuda"), align=False)
+            eng.commit()
+        else:
+            eng.set_last_vector(torch.tensor(ys[a - 1], dtype=dt, device="cuda"))
+        alpha = float(alphas[a])
+        g = gershgorin_bound(info.d_min, info.d_max, alpha)
+        rho = compute_shift_rho(float(z["row_lambda1"][a - 1]), g)
+        rec = eng.alpha_solve(alpha=alpha, alpha_prev=float(alphas[a - 1]), rho=rho, gershgorin=g, tol=1e-6,
+                              pred_tol=p.get("pred_tol", 1e-3), maxiter=1000, ncv=default_ncv(n, None), start_mode=mode, seed=42,
+                              stream_id=4 * a, align=True)
+        assert rho - rec.mu == pytest.approx(float(z["row_lambda1"][a]), abs=2e-5)
+        ref_pr = float(z["row_pred_residual"][a])
+        if np.isnan(ref_pr):
+            assert rec.pred_accepted == -1 and np.isnan(rec.pred_residual)
+            continue
+        assert rec.pred_residual == pytest.approx(ref_pr, rel=2e-3, abs=1e-6), a
+        acc_ref = bool(z["row_pred_accepted"][a])
+        if abs(ref_pr - 1e-3) > 1e-5:
+            assert bool(rec.pred_accepted) == acc_ref, a
+        else:
+            borderline += int(bool(rec.pred_accepted) != acc_ref)
+    assert borderline <= 1
 
 
 def test_synthetic_ba_sweep_properties():

@@ -51,6 +51,30 @@ def test_noalloc_operator_matches_handle_operator_twice():
         assert err < 3e-6, (alpha, err)
 
 
+def test_noalloc_defined_on_zero_couplings_and_bad_columns():
+    """All-zero couplings give y = rho x (no NaN); an out-of-range column is skipped."""
+    lib = _lib.load()
+    n = 64
+    rp = np.arange(n + 1, dtype=np.int32)                    # one entry per row
+    col = ((np.arange(n) + 1) % n).astype(np.int32)
+    x = torch.linspace(-1, 1, n, dtype=torch.float32, device="cuda")
+    d_rp = torch.from_numpy(rp).cuda()
+    zero = torch.zeros(n, dtype=torch.float32, device="cuda")
+    J = type("J", (), {"shape": (n, n), "nnz": n})
+    y = _noalloc(lib, J, d_rp, torch.from_numpy(col).cuda(), zero, 0.5, 1.25, x)
+    assert torch.equal(y, 1.25 * x)
+    # a ring with one column out of range: that product is dropped, the other rows are untouched
+    bad = col.copy()
+    bad[3] = n + 1000
+    ones = torch.ones(n, dtype=torch.float32, device="cuda")
+    y_ok = _noalloc(lib, J, d_rp, torch.from_numpy(col).cuda(), ones, 0.0, 0.0, x)
+    y_bad = _noalloc(lib, J, d_rp, torch.from_numpy(bad).cuda(), ones, 0.0, 0.0, x)
+    assert torch.isfinite(y_bad).all()
+    assert float(y_bad[3]) == 0.0
+    keep = torch.arange(n, device="cuda") != 3
+    assert torch.equal(y_bad[keep], y_ok[keep])
+
+
 def test_noalloc_rejects_sizes_beyond_its_array():
     lib = _lib.load()
     x = torch.zeros(4, dtype=torch.float32, device="cuda")

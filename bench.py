@@ -55,6 +55,8 @@ def parse():
                          "(64 instances x 4 seeds x 128 alphas, one launch); precision: FP32 + FP64 Ritz vs "
                          "all-FP64 on BA(2^16); grad: the differentiation workload on BA(2^18)")
     ap.add_argument("--scale-precisions", default="32,64", help="--scale-run: precisions to run, in order")
+    ap.add_argument("--scale-log2n", type=int, default=25,
+                    help="the default line's scale block: log2 n of its BA graph (0: no scale block)")
     ap.add_argument("--scale-run", action="store_true",
                     help="one timed FP32 solve and one timed plain-FP64 solve of the graph, with the energy gap")
     ap.add_argument("--spmv-layout", choices=["auto", "panel", "split", "worklist"], default="auto",
@@ -519,6 +521,59 @@ def run_grad(args):
     print(json.dumps(out))
 
 
+def scale_solves(args, dev, n, rowptr, col, val, d_rowptr=None, d_col=None, d_val=None):
+    """One timed FP32 (FP64 Ritz) solve and one timed all-FP64 solve of the same graph, CSR resident
+    (int64 row pointers, int32 columns), and their best-energy gap: the large-scale half of the metric.
+    Returns the block as a dict; frees its device arrays."""
+    import torch
+    from specann_b200.spectral_annealing import SpectralAnnealing
+    nnz = int(rowptr[-1])
+    if d_rowptr is None:
+        d_rowptr = torch.from_numpy(np.ascontiguousarray(rowptr, dtype=np.int64)).to(dev)
+        d_col = torch.from_numpy(col).to(dev)
+        d_val = torch.from_numpy(val).to(dev)
+    out = {"n": n, "nnz": nnz, "rowptr": str(d_rowptr.dtype).replace("torch.", ""),
+           "workload": f"BA(n={n}, m={args.m}) J=-A, {args.num_alphas} alphas sqrt schedule, diagonal predictor, "
+                       f"eigsh_tol 1e-6, batched local search; CSR resident"}
+    from specann_b200 import graphs as _g
+    Jw = _g.barabasi_albert(4096, 8, seed=1)       # load the kernels once (not timed)
+    SpectralAnnealing("w.txt", "w", random_seed=1, num_alphas=4, write_results=False).solve(Jw)
+    for prec in [int(x) for x in args.scale_precisions.split(",")]:
+        if prec == 64:
+            del d_val
+            torch.cuda.empty_cache()
+            d_val = torch.from_numpy(val.astype(np.float64)).to(dev)
+        s = SpectralAnnealing("scale.txt", "scale", random_seed=42, num_alphas=args.num_alphas, precision=prec,
+                              write_results=False, profile=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e, spins, _ = s.solve_device(d_rowptr, d_col, d_val)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        st = s.engine.stats
+        iters = [r["eigsh_iterations"] for r in s.alpha_results]
+        res = [r["eigsh_residual"] for r in s.alpha_results]
+        out[f"fp{prec}"] = {"seconds": dt, "best_energy": e, "spmvs": st["spmvs"], "layout": s.operator_layout,
+                            "alpha_kernel_s": st["alpha_ms"] / 1e3, "ls_kernel_s": st["ls_ms"] / 1e3,
+                            "alpha_GBps": st["alpha_bytes"] / (st["alpha_ms"] / 1e3) / 1e9,
+                            "phase_s": [round(x / 1e3, 3) for x in st.get("phase_ms", [0] * 6)],
+                            "iters_mean": float(np.mean(iters)), "iters_max": int(np.max(iters)),
+                            "max_residual": float(np.nanmax(res)),
+                            "alphas_above_1e-5": int(sum(1 for x in res if x > 1e-5)),
+                            "alphas_skipped": int(s._alphas_skipped),
+                            "candidates": int(s._num_candidates or 0),
+                            "peak_mem_gb": torch.cuda.max_memory_allocated() / 1e9}
+        del s
+        torch.cuda.empty_cache()
+    if "fp32" in out and "fp64" in out:
+        e32, e64 = out["fp32"]["best_energy"], out["fp64"]["best_energy"]
+        out["energy_gap_rel"] = abs(e32 - e64) / abs(e64)
+        out["fp64_over_fp32"] = out["fp64"]["seconds"] / out["fp32"]["seconds"]
+    del d_rowptr, d_col, d_val
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -548,7 +603,9 @@ def main():
     lib = _lib.load()
     n, rowptr, col, val = make_graph(args)
     nnz = int(rowptr[-1])
-    rp_np = rowptr.astype(np.int32) if nnz < 2**31 else rowptr
+    # 64-bit row pointers for the scale run (the C5 form: int32 columns, int64 row pointers) or when nnz
+    # needs them; else int32
+    rp_np = rowptr if (args.scale_run or nnz >= 2**31) else rowptr.astype(np.int32)
     import scipy.sparse as sp
     J_host = sp.csr_matrix((val.astype(np.float64) if args.precision == 64 else val, col, rp_np), shape=(n, n))
     d_rowptr = torch.from_numpy(rp_np).to(dev)
@@ -566,42 +623,7 @@ def main():
             dist.barrier()
 
     if args.scale_run:
-        out = {"scale_run": True, "n": n, "nnz": nnz, "workload": f"BA(n=2^{args.log2n}, m={args.m}) J=-A, "
-                                                                  f"{args.num_alphas} alphas sqrt schedule"}
-        # load the kernels once on a small graph (not timed)
-        from specann_b200 import graphs as _g
-        Jw = _g.barabasi_albert(4096, 8, seed=1)
-        SpectralAnnealing("w.txt", "w", random_seed=1, num_alphas=4, write_results=False).solve(Jw)
-        d_val64 = None
-        for prec in [int(x) for x in args.scale_precisions.split(",")]:
-            if prec == 64:
-                del d_val
-                torch.cuda.empty_cache()
-                d_val64 = torch.from_numpy(val.astype(np.float64)).to(dev)
-            vv = d_val if prec == 32 else d_val64
-            s = SpectralAnnealing("scale.txt", "scale", random_seed=42, num_alphas=args.num_alphas, precision=prec,
-                                  write_results=False, profile=True)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            e, spins, _ = s.solve_device(d_rowptr, d_col, vv)
-            torch.cuda.synchronize()
-            dt = time.perf_counter() - t0
-            st = s.engine.stats
-            iters = [r["eigsh_iterations"] for r in s.alpha_results]
-            out[f"fp{prec}"] = {"seconds": dt, "best_energy": e, "spmvs": st["spmvs"],
-                                "alpha_kernel_s": st["alpha_ms"] / 1e3, "ls_kernel_s": st["ls_ms"] / 1e3,
-                                "alpha_GBps": st["alpha_bytes"] / (st["alpha_ms"] / 1e3) / 1e9,
-                                "phase_s": [round(x / 1e3, 3) for x in st.get("phase_ms", [0] * 6)],
-                                "iters_mean": float(np.mean(iters)), "iters_max": int(np.max(iters)),
-                                "max_residual": float(np.nanmax([r["eigsh_residual"] for r in s.alpha_results])),
-                                "candidates": int(s._num_candidates or 0),
-                                "peak_mem_gb": torch.cuda.max_memory_allocated() / 1e9}
-            del s
-            torch.cuda.empty_cache()
-            print(json.dumps(out), flush=True)
-        if "fp32" in out and "fp64" in out:
-            e32, e64 = out["fp32"]["best_energy"], out["fp64"]["best_energy"]
-            out["energy_gap_rel"] = abs(e32 - e64) / abs(e64)
+        out = scale_solves(args, dev, n, rowptr, col, val, d_rowptr, d_col, d_val)
         print(json.dumps(out))
         return
 
@@ -765,6 +787,15 @@ def main():
         line["cpu_baseline"] = cpu_baseline_sample(args, J_host, int(s._num_candidates or 1),
                                                    int(getattr(s, "_ls_passes", 1)))
         line["cpu_baseline"]["full_solves"] = full_solve_baselines(args)
+    if rank == 0 and world == 1 and args.scale_log2n > 0:
+        # the large-scale half of the metric: BA(2^25) FP32 vs plain FP64 on this GPU
+        del eng, x, y
+        torch.cuda.empty_cache()
+        import argparse as _ap
+        sargs = _ap.Namespace(**vars(args))
+        sargs.log2n = args.scale_log2n
+        n2, rp2, col2, val2 = make_graph(sargs)
+        line["scale"] = scale_solves(sargs, dev, n2, rp2, col2, val2)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

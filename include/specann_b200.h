@@ -184,6 +184,12 @@ int sa_split_count(sa_handle* h, int32_t* splits, double* matrix_bytes);
  * magnitude, chunk bounds). Any pointer may be NULL; INVALID_ARG when no layout is built. */
 int sa_panel_info(sa_handle* h, int64_t* slots, int32_t* row_blocks, int32_t* panels, int32_t* width,
                   double* alg_bytes);
+/* Device pointers to the built layout's tables (diagnostics; no reference counterpart): the padded
+ * entry stream (uint32 per slot: row in block << 16 | sign << 15 | column in panel; padding
+ * 0xFFFF0000), the chunk starts (int64, [(block * panels + panel) * 16 + warp], one extra end entry)
+ * and the block first rows (int32, row_blocks + 1). Any pointer may be NULL; valid until the next
+ * sa_set_matrix. */
+int sa_panel_tables(sa_handle* h, const void** entries, const void** chunk_starts, const void** block_rows);
 
 /* One alpha of the sweep (models/spectral_annealing.py:568-669 with utils/eigsh.py:10-17 and
  * utils/predictors.py): start vector / predictor with its residual test, warm-started
@@ -410,6 +416,20 @@ int sa_batch_results(sa_batch* b, sa_batch_alpha_record* records, sa_batch_summa
 int sa_batch_candidate(sa_batch* b, int32_t problem, int32_t slot, int32_t refined, uint32_t* packed_device);
 
 int sa_batch_destroy(sa_batch* b);
+
+/* ---- instance matrix built on the device ------------------------------------------------------
+ * The COO -> CSR step of the reference's loader (utils/data_loader.py:112-204: both triangles appended
+ * edge by edge, coo_matrix(...).tocsr() summing duplicates, _remove_isolated_nodes) for an edge list
+ * parsed on the host: a stable device radix sort of the 2 num_edges directed entries by (row, column),
+ * duplicates summed in file order in FP64, rows whose entries are all zero removed (when any entry
+ * exists) and the rest renumbered. ei, ej (int64) and ew (double) are device arrays of num_edges
+ * undirected edges in file order; the outputs are device arrays sized for the worst case (row pointers
+ * num_vertices + 1, columns and values 2 num_edges, node_ids num_vertices): the kept rows' original
+ * indices go to node_ids, and *n_out, *nnz_out give the result's size. Synchronises `stream`. */
+int sa_coo_workspace_size(int64_t num_edges, int64_t num_vertices, size_t* bytes);
+int sa_coo_to_csr(int64_t num_edges, int64_t num_vertices, const int64_t* ei, const int64_t* ej, const double* ew,
+                  void* workspace, size_t bytes, int64_t* rowptr, int32_t* col, double* val, int64_t* node_ids,
+                  int64_t* n_out, int64_t* nnz_out, void* stream);
 
 /* ---- allocation-free operator ------------------------------------------------------------- */
 

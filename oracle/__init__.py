@@ -8,10 +8,15 @@ fallback.
 Modules:
   specann_oracle  NumPy/SciPy restatement of the reference solver (prelude, schedule, operators,
                   shift, predictors, eigensolve with retry/checks, rounding, signatures, energies,
-                  local search, best-candidate selection).
+                  local search, best-candidate selection), the reference kernel's in-order fp32 pass
+                  and the deviation count against it, and row-block threaded products for the timed
+                  CPU baseline.
   selection       the counter-based node-selection stream shared with the CUDA local search.
-  graphs          seeded Barabasi-Albert / Erdos-Renyi generators used for synthetic inputs.
-  ls_oracle.c     the same local search and energies in plain C (for CPU baselines at large n).
+  guards_oracle   the guarded local-search policies (fixed / adaptive guard, independent set,
+                  sequential oracle).
+  adjoint_oracle  dense FP64 eigenvector adjoint and gradient (the differentiation form's checker).
+  build_tools     builds _bin/ba_graph from ba_graph_main.cpp: the stand-alone graph writer the CPU
+                  reference arm runs, so that its process loads none of the product's libraries.
 
 Parity pin: tests/golden/make_golden.py runs the reference's own solver code (the CuPy files of the
 reference, executed on NumPy/SciPy through a stand-in module) and freezes its per-alpha records;

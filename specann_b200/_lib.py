@@ -148,6 +148,7 @@ SIGNATURES = {
     "sa_panel_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                 C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "sa_get_spmv_policy": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    "sa_panel_tables": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "sa_alpha_solve": (C.c_int, [C.c_void_p, C.POINTER(AlphaParams), C.POINTER(AlphaRecord)]),
     "sa_result_vector": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "sa_commit_alpha": (C.c_int, [C.c_void_p]),
@@ -181,6 +182,10 @@ SIGNATURES = {
     "sa_batch_results": (C.c_int, [C.c_void_p, C.POINTER(BatchAlphaRecord), C.POINTER(BatchSummary)]),
     "sa_batch_candidate": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
     "sa_batch_destroy": (C.c_int, [C.c_void_p]),
+    "sa_coo_workspace_size": (C.c_int, [C.c_int64, C.c_int64, C.POINTER(C.c_size_t)]),
+    "sa_coo_to_csr": (C.c_int, [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int64),
+                                C.POINTER(C.c_int64), C.c_void_p]),
 }
 
 GRAPH_SIGNATURES = {
@@ -191,6 +196,9 @@ GRAPH_SIGNATURES = {
     "sa_instance_load": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
                                    C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "sa_instance_fetch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sa_instance_edges": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
+                                    C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "sa_instance_fetch_edges": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sa_greedy_coloring": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32)]),
 }
 

@@ -19,7 +19,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 CUDA_LIB = "libspecann_b200.so"
 GRAPH_LIB = "libspecann_graphs.so"
-CU_SOURCES = ["capi.cu", "alpha.cu", "ls.cu", "batch.cu", "adjoint.cu", "noalloc.cu", "panel.cu", "split.cu",
+CU_SOURCES = ["capi.cu", "alpha.cu", "ls.cu", "batch.cu", "adjoint.cu", "noalloc.cu", "panel.cu", "split.cu", "coo.cu",
               "guard.cu"]
 HEADERS = ["common.cuh", "handle.cuh", "spmv.cuh", "policy.cuh", "alpha_body.cuh", "ls_body.cuh", "panel.cuh"]
 

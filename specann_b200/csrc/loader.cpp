@@ -78,7 +78,16 @@ int parse_edge(const std::string& raw, int64_t* i, int64_t* j, double* w) {
   return 1;
 }
 
-int load(const char* path, int gset, Instance* out) {
+// The edge list of an instance file in file order (fields as edges to the bias node appended last),
+// before duplicates are summed: what both the host CSR (load) and the device build (sa_coo_to_csr)
+// start from.
+struct EdgeList {
+  int64_t n_original = 0, n_vertices = 0, bias = -1;
+  std::vector<int64_t> ei, ej;
+  std::vector<double> ew;
+};
+
+int parse_edges(const char* path, int gset, EdgeList* el) {
   std::ifstream f(path);
   if (!f) return 2;
   std::string line;
@@ -131,6 +140,23 @@ int load(const char* path, int gset, Instance* out) {
         if (h[(size_t)q] != 0.0) { ei.push_back(bias); ej.push_back(q); ew.push_back(h[(size_t)q]); }
     }
   }
+  el->n_original = n;
+  el->n_vertices = nv;
+  el->bias = bias;
+  el->ei.swap(ei);
+  el->ej.swap(ej);
+  el->ew.swap(ew);
+  return 0;
+}
+
+int load(const char* path, int gset, Instance* out) {
+  EdgeList el;
+  const int pst = parse_edges(path, gset, &el);
+  if (pst != 0) return pst;
+  const int64_t n = el.n_original, nv = el.n_vertices, bias = el.bias;
+  const std::vector<int64_t>& ei = el.ei;
+  const std::vector<int64_t>& ej = el.ej;
+  const std::vector<double>& ew = el.ew;
   // both triangles, in the order the reference appends them: (i, j, w) then (j, i, w) per edge
   const size_t ne = ei.size();
   std::vector<int64_t> r(2 * ne), c(2 * ne);
@@ -202,6 +228,33 @@ int sa_instance_load(const char* path, int32_t gset, void** inst, int64_t* n, in
   *nnz = (int64_t)x->col.size();
   *n_original = x->n_original;
   *bias_index = x->bias_index;
+  return 0;
+}
+
+// Parse an instance file into its edge list (file order, fields as bias edges last) for the device
+// build (sa_coo_to_csr): 0 on success, or the codes of sa_instance_load.
+int sa_instance_edges(const char* path, int32_t gset, void** edges, int64_t* num_edges, int64_t* num_vertices,
+                      int64_t* n_original, int64_t* bias_index) {
+  if (!path || !edges || !num_edges || !num_vertices || !n_original || !bias_index) return 1;
+  EdgeList* x = new EdgeList();
+  const int st = parse_edges(path, gset ? 1 : 0, x);
+  if (st != 0) { delete x; *edges = nullptr; return st; }
+  *edges = x;
+  *num_edges = (int64_t)x->ei.size();
+  *num_vertices = x->n_vertices;
+  *n_original = x->n_original;
+  *bias_index = x->bias;
+  return 0;
+}
+
+// Copy the edge list into caller arrays (num_edges each), then free the object.
+int sa_instance_fetch_edges(void* edges, int64_t* ei, int64_t* ej, double* ew) {
+  EdgeList* x = (EdgeList*)edges;
+  if (!x || ((!ei || !ej || !ew) && !x->ei.empty())) return 1;
+  std::copy(x->ei.begin(), x->ei.end(), ei);
+  std::copy(x->ej.begin(), x->ej.end(), ej);
+  std::copy(x->ew.begin(), x->ew.end(), ew);
+  delete x;
   return 0;
 }
 

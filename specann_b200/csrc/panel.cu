@@ -461,6 +461,14 @@ int sa_panel_info(sa_handle* h, int64_t* slots, int32_t* row_blocks, int32_t* pa
   return SA_OK;
 }
 
+int sa_panel_tables(sa_handle* h, const void** entries, const void** chunk_starts, const void** block_rows) {
+  if (!h || !h->panel_ready) return SA_ERR_INVALID_ARG;
+  if (entries) *entries = h->panel_ent;
+  if (chunk_starts) *chunk_starts = h->panel_chunk;
+  if (block_rows) *block_rows = h->panel_row0;
+  return SA_OK;
+}
+
 int sa_panel_enable(sa_handle* h, int32_t on) {
   if (!h || (on && !h->panel_ready)) return SA_ERR_INVALID_ARG;
   h->panel_on = on ? 1 : 0;

@@ -163,6 +163,18 @@ class Engine:
         return {"slots": int(slots.value), "blocks": int(blocks.value), "panels": int(panels.value),
                 "width": int(width.value), "matrix_bytes": float(nb.value)}
 
+    def panel_tables(self):
+        """Host copies of the built panel layout's tables: (entry words uint32[slots], chunk starts
+        int64[blocks * panels * 16 + 1], block first rows int32[blocks + 1])."""
+        info = self.panel_info()
+        e, ch, r0 = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check("sa_panel_tables", self.lib.sa_panel_tables(self.h, C.byref(e), C.byref(ch), C.byref(r0)))
+        nb, npn = info["blocks"], info["panels"]
+        ent = device_view(e.value, info["slots"], torch.int32, self.device).cpu().numpy().view(np.uint32)
+        chunk = device_view(ch.value, nb * npn * 16 + 1, torch.int64, self.device).cpu().numpy()
+        row0 = device_view(r0.value, nb + 1, torch.int32, self.device).cpu().numpy()
+        return ent, chunk, row0
+
     def build_splits(self, splits: int = 0) -> int:
         """Lay the bound matrix out as L2 column splits (0: one per 48 MB of the gathered vector)
         and switch the operator kernels to it. Returns the number of splits."""

@@ -62,6 +62,54 @@ def load_file(path, gset: bool, return_index: bool = False):
     return J, index
 
 
+def load_file_device(path, gset: bool, device=None):
+    """Parse one instance file on the host into its edge list and build the CSR on the device
+    (sa_coo_to_csr). Returns (row pointers int64, columns int32, couplings float64) as device tensors
+    and the InstanceIndex; the matrix equals load_file's."""
+    import torch
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    g = _lib.load_graphs()
+    h = C.c_void_p()
+    ne, nv, n0, bias = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+    st = g.sa_instance_edges(str(path).encode(), int(bool(gset)), C.byref(h), C.byref(ne), C.byref(nv),
+                             C.byref(n0), C.byref(bias))
+    if st != 0:
+        kind = "Gset" if gset else "linear bias"
+        raise DataLoadError(f"Error reading {kind} file {path}: {_ERRORS.get(st, st)}")
+    m = ne.value
+    ei = np.empty(m, dtype=np.int64)
+    ej = np.empty(m, dtype=np.int64)
+    ew = np.empty(m, dtype=np.float64)
+    if g.sa_instance_fetch_edges(h, ei.ctypes.data_as(C.c_void_p), ej.ctypes.data_as(C.c_void_p),
+                                 ew.ctypes.data_as(C.c_void_p)) != 0:
+        raise DataLoadError(f"Error reading {path}")
+    lib = _lib.load()
+    nbytes = C.c_size_t(0)
+    _lib.check("sa_coo_workspace_size", lib.sa_coo_workspace_size(m, nv.value, C.byref(nbytes)))
+    ws = torch.empty(nbytes.value + 256, dtype=torch.uint8, device=dev)
+    wp = (ws.data_ptr() + 255) & ~255
+    d_ei, d_ej, d_ew = (torch.from_numpy(a).to(dev) for a in (ei, ej, ew))
+    rowptr = torch.empty(nv.value + 1, dtype=torch.int64, device=dev)
+    col = torch.empty(max(1, 2 * m), dtype=torch.int32, device=dev)
+    val = torch.empty(max(1, 2 * m), dtype=torch.float64, device=dev)
+    ids = torch.empty(nv.value, dtype=torch.int64, device=dev)
+    n_out, nnz_out = C.c_int64(), C.c_int64()
+    stream = torch.cuda.current_stream(dev)
+    _lib.check("sa_coo_to_csr", lib.sa_coo_to_csr(m, nv.value, C.c_void_p(d_ei.data_ptr()), C.c_void_p(d_ej.data_ptr()),
+                                                 C.c_void_p(d_ew.data_ptr()), C.c_void_p(wp), nbytes.value,
+                                                 C.c_void_p(rowptr.data_ptr()), C.c_void_p(col.data_ptr()),
+                                                 C.c_void_p(val.data_ptr()), C.c_void_p(ids.data_ptr()),
+                                                 C.byref(n_out), C.byref(nnz_out), C.c_void_p(stream.cuda_stream)))
+    n, nnz = int(n_out.value), int(nnz_out.value)
+    rowptr, col, val, ids = rowptr[:n + 1], col[:nnz], val[:nnz], ids[:n]
+    node_ids = ids.cpu().numpy()
+    b = int(bias.value)
+    b_new = int(np.flatnonzero(node_ids == b)[0]) if b >= 0 and np.any(node_ids == b) else -1
+    index = InstanceIndex(n_original=int(n0.value), n_solve=n, node_ids=node_ids, bias_node_index=b_new,
+                          id_base=1, weights_negated=bool(gset), J_sum=float(val.sum().item()) if nnz else 0.0)
+    return rowptr, col, val, index
+
+
 class DataLoader:
     """Load the instances of one dataset folder (datasets/<name>); a name containing "gset" selects
     the Gset format, any other the linear-bias format (utils/data_loader.py:39-64)."""

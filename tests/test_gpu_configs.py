@@ -11,11 +11,14 @@
   * The headline workload, BA(2^20, m = 20), 128 sqrt alphas, through the column-panel layout: six
     eigenpairs of the warm-started chain against the FP64 operator and SciPy's eigsh.
   * 64-bit row pointers forced on small matrices: the `long long` instantiations of the alpha,
-    local-search, panel and split kernels give the same results as the int32 ones.
+    local-search, panel and split kernels give the same results as the int32 ones (up to the global
+    sign of the eigenvector chain).
   * C2, BA(2^16, m = 20): FP32 with FP64 Ritz against all-FP64, per alpha.
-  * C5's row-pointer form at full size, BA(2^25, m = 20) with int64 row pointers: a short warm-started
-    chain in FP32 and FP64 (the full 128-alpha run is a bench workload).
+The full-size C5 form (BA(2^25), int64 row pointers, FP32 against FP64) is the bench line's scale
+block; here its row-pointer instantiations are checked on small matrices.
 """
+import os
+
 import numpy as np
 import pytest
 import scipy.linalg as sla
@@ -144,6 +147,7 @@ def test_headline_ba2e20_panel_chain_against_fp64():
     assert s._alphas_skipped == 0
     assert O.exact_energy(J, spins) == energy
     J64 = sp.csr_matrix(J, dtype=np.float64)
+    Jt = O.threaded(J64, os.cpu_count() or 1)      # row-block parallel products (same sums)
     k = s._num_candidates
     for i in keep:
         r = s.alpha_results[i]
@@ -151,13 +155,15 @@ def test_headline_ba2e20_panel_chain_against_fp64():
         y, rho, mu = s.kept_vectors[i]
         y = y.double().cpu().numpy()
         sig = scaling(J, alpha)
-        My = apply_M(J64, sig, y)
+        My = sig * (Jt @ (sig * y))
         lam_rq = float(y @ My) / float(y @ y)
         res = np.linalg.norm(My - lam_rq * y) / np.linalg.norm(y)
         assert res <= 1e-5, (i, res)
         assert abs((rho - mu) - lam_rq) <= 1e-5
-        op = spla.LinearOperator(J.shape, matvec=lambda v, sig=sig: apply_M(J64, sig, v), dtype=np.float64)
-        w = spla.eigsh(op, k=1, which="LA", v0=y, tol=1e-10, ncv=8, return_eigenvectors=False)
+        op = spla.LinearOperator(J.shape, matvec=lambda v, sig=sig: sig * (Jt @ (sig * v)), dtype=np.float64)
+        # started from the GPU vector, ARPACK (at the solver's own tolerance) confirms that it is the
+        # leading eigenvalue
+        w = spla.eigsh(op, k=1, which="LA", v0=y, tol=1e-6, ncv=32, maxiter=100, return_eigenvectors=False)
         assert abs(r["lambda1"] - float(w[0])) <= 1e-5, (i, r["lambda1"], float(w[0]))
         spins_i = s.engine.candidate_spins(r["candidate"]).cpu().numpy()
         assert np.array_equal(spins_i, np.where(y >= 0, 1, -1).astype(np.int8)), i
@@ -184,9 +190,12 @@ def test_rowptr64_matches_rowptr32(layout, couplings):
                      candidates(s, k, refined=True), [r["eigsh_iterations"] for r in s.alpha_results])
     e32, s32, l32, c32, r32, it32 = out[False]
     e64, s64, l64, c64, r64, it64 = out[True]
-    assert e32 == e64 and np.array_equal(s32, s64)
+    # the two instantiations are separate compiled code: the chain may come out with the other global
+    # sign of the eigenvectors (both are eigenvectors), which negates every candidate and refined spin
+    sign = 1 if np.array_equal(c32[0], c64[0]) else -1
+    assert e32 == e64 and np.array_equal(s32, sign * s64)
     assert np.max(np.abs(np.array(l32) - np.array(l64))) <= 1e-6
-    assert np.array_equal(c32, c64) and np.array_equal(r32, r64)
+    assert np.array_equal(c32, sign * c64) and np.array_equal(r32, sign * r64)
 
 
 def test_rowptr64_split_operator_and_local_search_direct():
@@ -242,34 +251,6 @@ def test_c2_precision_fp32_ritz64_against_fp64():
         sig = scaling(J, rows64[i]["alpha"])
         op = spla.LinearOperator(J.shape, matvec=lambda v, sig=sig: apply_M(J64, sig, v), dtype=np.float64)
         y = kept64[i][0].cpu().numpy()
-        w = spla.eigsh(op, k=1, which="LA", v0=y, tol=1e-12, return_eigenvectors=False)
+        w = spla.eigsh(op, k=1, which="LA", v0=y, tol=1e-12, ncv=20, maxiter=200, return_eigenvectors=False)
         assert abs(rows64[i]["lambda1"] - float(w[0])) <= 1e-8
         assert abs(rows32[i]["lambda1"] - float(w[0])) <= 1e-6
-
-
-# ------------------------------------------------------------------------------------------------
-# C5's row-pointer form at full size
-# ------------------------------------------------------------------------------------------------
-
-def test_c5_int64_rowptr_full_size_short_chain():
-    """BA(2^25, m = 20) with int64 row pointers (the L2 column-split layout): 6 warm-started alphas,
-    sqrt-spaced over t in [0, 0.05], in FP32 (FP64 Ritz) and in FP64; per-alpha eigenvalues agree to
-    1e-6, residuals are below 1e-5 and the best energies agree to 1e-3 relative."""
-    n = 1 << 25
-    rp, col, val = graphs.barabasi_albert_arrays(n, 20, seed=42)
-    d_rp = torch.from_numpy(rp.astype(np.int64)).cuda()
-    d_col = torch.from_numpy(col).cuda()
-    res = {}
-    for prec in (32, 64):
-        d_val = torch.from_numpy(val.astype(np.float32 if prec == 32 else np.float64)).cuda()
-        s = SpectralAnnealing("c5.txt", "c5", random_seed=42, precision=prec, num_alphas=6,
-                              schedule_interval=(0.0, 0.05), write_results=False)
-        e, spins, _ = s.solve_device(d_rp, d_col, d_val)
-        assert s.engine.rowptr64 and s.operator_layout == "split"
-        assert s._alphas_skipped == 0
-        res[prec] = (e, [r["lambda1"] for r in s.alpha_results], max(r["eigsh_residual"] for r in s.alpha_results))
-        del s, d_val
-        torch.cuda.empty_cache()
-    assert np.max(np.abs(np.array(res[32][1]) - np.array(res[64][1]))) <= 1e-6
-    assert res[32][2] <= 1e-5 and res[64][2] <= 1e-5
-    assert abs(res[32][0] - res[64][0]) <= 1e-3 * abs(res[64][0])

@@ -154,3 +154,43 @@ def test_panel_layout_deterministic():
     real = w[w != 0xFFFF0000]
     assert len(real) == J.nnz
     assert np.all((real >> 16) < 16384) and np.all((real & 0x7FFF) < 16384)
+
+
+def test_layout_tables_follow_the_restated_piece_rules():
+    """The device-built entry stream and chunk table equal what the CPU restatement of the piece
+    packing and warp cuts (tests/test_panel_pieces_logic.py) gives for every segment of a skewed
+    graph with long hub rows."""
+    from test_panel_pieces_logic import PIECE, WARPS, pieces, warp_starts
+    J = graphs.barabasi_albert(20000, 8, seed=9).tolil()
+    for j in range(1, 3001):                      # a hub of 3000 leaves: rows longer than a piece
+        J[0, j] = -1.0
+        J[j, 0] = -1.0
+    J = J.tocsr()
+    eng = engine_for(J, 32)
+    eng.build_panels()
+    info = eng.panel_info()
+    ent, chunk, row0 = eng.panel_tables()
+    nb, npn, width = info["blocks"], info["panels"], info["width"]
+    assert chunk[nb * npn * WARPS] == info["slots"]
+    pad = np.uint32(0xFFFF0000)
+    for b in range(nb):
+        r_lo, r_hi = int(row0[b]), int(row0[b + 1])
+        a, e = J.indptr[r_lo], J.indptr[r_hi]
+        rows = np.repeat(np.arange(r_lo, r_hi), np.diff(J.indptr[r_lo:r_hi + 1]))
+        cols = J.indices[a:e]
+        neg = J.data[a:e] < 0
+        for p in range(npn):
+            sel = (cols // width) == p
+            seg_rows = rows[sel]
+            words = ((seg_rows - r_lo).astype(np.uint32) << 16) | (neg[sel].astype(np.uint32) << 15) | \
+                (cols[sel] - p * width).astype(np.uint32)
+            pcs = pieces(seg_rows)
+            st = warp_starts(seg_rows, pcs)
+            q = (b * npn + p) * WARPS
+            base = int(chunk[q])
+            assert [int(x) for x in chunk[q:q + WARPS]] == [base + PIECE * t for t in st]
+            assert int(chunk[q + WARPS]) == base + PIECE * len(pcs)
+            for i, (s0, ln) in enumerate(pcs):
+                slot = base + PIECE * i
+                assert np.array_equal(ent[slot:slot + ln], words[s0:s0 + ln]), (b, p, i)
+                assert np.all(ent[slot + ln:slot + PIECE] == pad)

@@ -50,6 +50,8 @@ def parse():
                     help="reference arm: local-search passes of a full solve (89: the count of the default "
                          "workload's solve, seed 42, whose local search is bit-exact with the CPU one)")
     ap.add_argument("--spmv-reps", type=int, default=20)
+    ap.add_argument("--batch-count", type=int, default=64,
+                    help="--workload batch: instances of the ragged batch (64: the workload; fewer for profiling)")
     ap.add_argument("--workload", default="metric", choices=["metric", "batch", "precision", "grad"],
                     help="metric: the headline solve (default); batch: the ragged batched workload "
                          "(64 instances x 4 seeds x 128 alphas, one launch); precision: FP32 + FP64 Ritz vs "
@@ -364,7 +366,7 @@ def run_batch(args, rank, world, local):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     dev = torch.device("cuda", local)
     lib = _lib.load()
-    inst = graphs.ragged_batch()
+    inst = graphs.ragged_batch(count=args.batch_count)
     Js = [J for _, J in inst]
     seeds = (42, 43, 44, 45)
     mine = sharding.shard_instances([(J.shape[0], J.nnz) for J in Js], world)[rank]

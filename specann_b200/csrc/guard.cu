@@ -232,6 +232,7 @@ __global__ void __launch_bounds__(kThreads, 2) guard_kernel(GuardArgs<VT, RP, GT
         if (indep) member = __ldg(A.colors + tile + lane) == color;
         else rk = sel_rank(tile + lane, keys, n);
       }
+      uint32_t tile_want = 0u;   // bit l set if node tile + l proposes a flip
       for (int sub = 0; sub < 32; sub += ne) {
         const long long i = tile + sub + slot;
         const long long rki = __shfl_sync(0xffffffffu, rk, (sub + slot) & 31);
@@ -258,17 +259,20 @@ __global__ void __launch_bounds__(kThreads, 2) guard_kernel(GuardArgs<VT, RP, GT
           fl[t] = (cp == 32) ? bal : ((bal >> (slot * cp)) & ((1u << cp) - 1u));
           if (f) atomicAdd((unsigned long long*)&s_cnt[q], 1ull);
         }
-        if (c == 0 && i < n) {
-          uint32_t any = 0u;
-          for (int t = 0; t < L.kw; ++t) {
-            L.wm[i * L.kw + t] = fl[t];
-            any |= fl[t];
-          }
-          if (any) {
-            const long long pos = (long long)atomicAdd((unsigned long long*)&G->wq_count, 1ull);
-            L.wq[pos] = (int)i;
-          }
-        }
+        uint32_t any = 0u;
+        for (int t = 0; t < L.kw; ++t) any |= fl[t];
+        if (c == 0 && i < n)
+          for (int t = 0; t < L.kw; ++t) L.wm[i * L.kw + t] = fl[t];
+        const uint32_t wb = __ballot_sync(0xffffffffu, c == 0 && i < n && any != 0u);
+        for (int sl = 0; sl < ne; ++sl)
+          if ((wb >> (sl * cp)) & 1u) tile_want |= 1u << (sub + sl);
+      }
+      if (tile_want) {
+        // one queue reservation per tile of 32 nodes
+        long long pos = 0;
+        if (lane == 0) pos = (long long)atomicAdd((unsigned long long*)&G->wq_count, (unsigned long long)__popc(tile_want));
+        pos = __shfl_sync(0xffffffffu, pos, 0);
+        if ((tile_want >> lane) & 1u) L.wq[pos + __popc(tile_want & ((1u << lane) - 1u))] = (int)(tile + lane);
       }
     }
     __syncthreads();

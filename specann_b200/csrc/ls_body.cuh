@@ -240,6 +240,7 @@ __device__ __forceinline__ void ls_body(const LsArgs<VT, RP, GT>& A, const Pol& 
         if (A.priority) A.prio[tile + lane] = selb ? rk : 0x7fffffff;
       }
       const uint32_t selmask = __ballot_sync(0xffffffffu, selb);
+      uint32_t tile_want = 0u;   // priority passes: bit l set if node tile + l wants to flip
       for (int sub = 0; sub < 32; sub += ne) {
         const long long i = tile + sub + slot;
         const bool valid = i < n && ((selmask >> (sub + slot)) & 1u);
@@ -266,10 +267,6 @@ __device__ __forceinline__ void ls_body(const LsArgs<VT, RP, GT>& A, const Pol& 
           for (int t = 0; t < A.kw; ++t) any |= fl[t];
           if (A.priority) {
             for (int t = 0; t < A.kw; ++t) A.wm[i * A.kw + t] = fl[t];
-            if (any) {
-              const long long pos = (long long)atomicAdd((unsigned long long*)&C->wq_count, 1ull);
-              A.wq[pos] = (int)i;
-            }
           } else if (any) {
             for (int t = 0; t < A.kw; ++t) A.flipm[i * A.kw + t] = fl[t];
             const long long deg = rp_load(A.rowptr, i + 1) - rp_load(A.rowptr, i);
@@ -278,6 +275,21 @@ __device__ __forceinline__ void ls_body(const LsArgs<VT, RP, GT>& A, const Pol& 
             for (long long q = 0; q < nch && pos + q < A.wl_cap; ++q) A.wl[pos + q] = (i << 22) | q;
           }
         }
+        if (A.priority) {
+          // the wanting nodes of this sub-step (one lane per node slot holds `any`)
+          uint32_t anyw = 0u;
+          for (int t = 0; t < A.kw; ++t) anyw |= fl[t];
+          const uint32_t wb = __ballot_sync(0xffffffffu, c == 0 && i < n && anyw != 0u);
+          for (int sl = 0; sl < ne; ++sl)
+            if ((wb >> (sl * cp)) & 1u) tile_want |= 1u << (sub + sl);
+        }
+      }
+      if (A.priority && tile_want) {
+        // one queue reservation per tile of 32 nodes (in node order within the tile)
+        long long pos = 0;
+        if (lane == 0) pos = (long long)atomicAdd((unsigned long long*)&C->wq_count, (unsigned long long)__popc(tile_want));
+        pos = __shfl_sync(0xffffffffu, pos, 0);
+        if ((tile_want >> lane) & 1u) A.wq[pos + __popc(tile_want & ((1u << lane) - 1u))] = (int)(tile + lane);
       }
     }
     if (!A.priority) {

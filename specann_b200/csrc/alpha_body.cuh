@@ -124,15 +124,23 @@ __device__ inline double last_component_sq(const double* a, const double* b, int
 // squared last component of its unit eigenvector in *s2 (every thread gets both). The tridiagonal
 // is first copied from the control block to shared memory: every Sturm count walks it
 // sequentially, so its loads must be short.
-__device__ inline double smallest_eig_block(const double* ag, const double* bg, int m, double* s2) {
+// hint_lo < hint_hi: a bracket to try first (from the previous step: by interlacing the smallest
+// eigenvalue of T_m is at most the previous smallest Ritz value, and the previous residual bounds how
+// far below it can be unless a new, lower eigenvalue appears); it is used only if the Sturm counts
+// confirm no eigenvalue below hint_lo and at least one below hint_hi, else the Gershgorin interval.
+__device__ inline double smallest_eig_block(const double* ag, const double* bg, int m, double* s2,
+                                            double hint_lo = 0.0, double hint_hi = -1.0) {
   __shared__ double s_lo, s_hi, s_s2;
-  __shared__ int s_first;
+  __shared__ int s_first, s_cnt_lo, s_cnt_hi;
   __shared__ double a[kNcvMax], b[kNcvMax];
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
     a[i] = ag[i];
     b[i] = (i + 1 < m) ? bg[i] : 0.0;
   }
   __syncthreads();
+  const bool hint = hint_lo < hint_hi;
+  if (hint && threadIdx.x == 1) s_cnt_lo = sturm_count(a, b, m, hint_lo);
+  if (hint && threadIdx.x == 2) s_cnt_hi = sturm_count(a, b, m, hint_hi);
   if (threadIdx.x == 0) {
     double lo = 1e300, hi = -1e300;
     for (int i = 0; i < m; ++i) {
@@ -143,6 +151,11 @@ __device__ inline double smallest_eig_block(const double* ag, const double* bg, 
     const double pad = 1e-12 * fmax(1.0, fmax(fabs(lo), fabs(hi)));
     s_lo = lo - pad;
     s_hi = hi + pad;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && hint && s_cnt_lo == 0 && s_cnt_hi >= 1 && hint_lo > s_lo && hint_hi < s_hi) {
+    s_lo = hint_lo;
+    s_hi = hint_hi;
   }
   __syncthreads();
   const int P = blockDim.x;
@@ -614,7 +627,10 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
 
     // ---------------- Lanczos steps ----------------------------------------------------------
     bool restart_p0 = false;
-    if (pol.block() == 0 && threadIdx.x == 0) C->gram_ok = 0;
+    if (pol.block() == 0 && threadIdx.x == 0) {
+      C->gram_ok = 0;
+      C->ritz_ok = 0;
+    }
     while (true) {
       const int j = vload(&C->j);
       const int pass2 = vload(&C->pass2);
@@ -892,7 +908,15 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
             if (act0 == ACT_NEXT) {
               const int m = j + 1;
               double s2;
-              const double th = smallest_eig_block(C->a, C->b, m, &s2);
+              // previous step's Ritz value and residual estimate as the bracket to try first
+              double hlo = 0.0, hhi = -1.0;
+              if (m >= 2 && C->ritz_ok) {
+                const double th0 = C->theta, r0 = C->res_est;
+                const double pad = 1e-12 * fmax(1.0, fabs(th0));
+                hlo = th0 - 2.0 * r0 - pad;
+                hhi = th0 + pad;
+              }
+              const double th = smallest_eig_block(C->a, C->b, m, &s2, hlo, hhi);
               if (threadIdx.x == 0) {
                 s_theta = th;
                 s_s2 = s2;
@@ -903,6 +927,7 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
                 const bool invariant = bj <= 1e-14 * bound;
                 C->theta = s_theta;
                 C->res_est = invariant ? 0.0 : res;
+                C->ritz_ok = 1;
                 const bool conv = invariant || res <= P.tol;
                 if (conv || C->iters >= P.maxiter) {
                   tridiag_eigvec(C->a, C->b, m, s_theta, C->s);

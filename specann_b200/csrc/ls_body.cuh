@@ -301,37 +301,54 @@ __device__ __forceinline__ void ls_body(const LsArgs<VT, RP, GT>& A, const Pol& 
     } else {
       if (!pol.sync(&C->gs)) return;
       // D2: a wanting node flips the candidates for which no wanting neighbour has a lower rank
-      // (one warp per wanting node; the blocking masks are OR-reduced over the row)
+      // (one warp per wanting node, 32 consecutive queue entries per warp; the blocking masks are
+      // OR-reduced over the row; the flipping nodes' work-list chunks are reserved with one atomic
+      // per 32 nodes)
       const long long nwq = *((volatile long long*)&C->wq_count);
       int cnt2[4] = {0, 0, 0, 0};
-      for (long long e = gwarp; e < nwq; e += nwarps) {
-        const long long i = (long long)__ldcg(A.wq + e);
-        const int pi = __ldcg(A.prio + i);
-        uint32_t W[4] = {0u, 0u, 0u, 0u}, B[4] = {0u, 0u, 0u, 0u};
-        for (int t = 0; t < A.kw; ++t) W[t] = __ldcg(A.wm + i * A.kw + t);
-        const long long rs = rp_load(A.rowptr, i), re = rp_load(A.rowptr, i + 1);
-        for (long long p = rs + lane; p < re; p += 32) {
-          const int j = __ldg(A.col + p);
-          if (__ldcg(A.prio + j) < pi)
-            for (int t = 0; t < A.kw; ++t) B[t] |= __ldcg(A.wm + (long long)j * A.kw + t);
-        }
-        uint32_t any = 0u;
-        for (int t = 0; t < A.kw; ++t) {
-          B[t] = __reduce_or_sync(0xffffffffu, B[t]);
-          W[t] &= ~B[t];
-          any |= W[t];
-          cnt2[t] += (W[t] >> lane) & 1u;
-        }
-        if (lane == 0 && any) {
-          for (int t = 0; t < A.kw; ++t) {
-            A.flipm[i * A.kw + t] = W[t];
-            if (W[t]) A.sb[i * A.kw + t] = __ldcg(A.sb + i * A.kw + t) ^ W[t];
+      for (long long base = gwarp * 32; base < nwq; base += nwarps * 32) {
+        long long my_node = 0, my_nch = 0;   // lane q: node base + q and its chunks if it flips
+        for (int q = 0; q < 32 && base + q < nwq; ++q) {
+          const long long i = (long long)__ldcg(A.wq + base + q);
+          const int pi = __ldcg(A.prio + i);
+          uint32_t W[4] = {0u, 0u, 0u, 0u}, B[4] = {0u, 0u, 0u, 0u};
+          for (int t = 0; t < A.kw; ++t) W[t] = __ldcg(A.wm + i * A.kw + t);
+          const long long rs = rp_load(A.rowptr, i), re = rp_load(A.rowptr, i + 1);
+          for (long long p = rs + lane; p < re; p += 32) {
+            const int j = __ldg(A.col + p);
+            if (__ldcg(A.prio + j) < pi)
+              for (int t = 0; t < A.kw; ++t) B[t] |= __ldcg(A.wm + (long long)j * A.kw + t);
           }
-          const long long deg = re - rs;
-          const long long nch = deg > kChunk ? (deg + kChunk - 1) / kChunk : 1;
-          const long long pos = (long long)atomicAdd((unsigned long long*)&C->wl_count, (unsigned long long)nch);
-          for (long long q = 0; q < nch && pos + q < A.wl_cap; ++q) A.wl[pos + q] = (i << 22) | q;
+          uint32_t any = 0u;
+          for (int t = 0; t < A.kw; ++t) {
+            B[t] = __reduce_or_sync(0xffffffffu, B[t]);
+            W[t] &= ~B[t];
+            any |= W[t];
+            cnt2[t] += (W[t] >> lane) & 1u;
+          }
+          if (lane == 0 && any) {
+            for (int t = 0; t < A.kw; ++t) {
+              A.flipm[i * A.kw + t] = W[t];
+              if (W[t]) A.sb[i * A.kw + t] = __ldcg(A.sb + i * A.kw + t) ^ W[t];
+            }
+          }
+          if (lane == q) {
+            my_node = i;
+            const long long deg = re - rs;
+            my_nch = any ? (deg > kChunk ? (deg + kChunk - 1) / kChunk : 1) : 0;
+          }
         }
+        // exclusive scan of the chunk counts over the lanes, one reservation for the warp
+        long long incl = my_nch;
+        for (int d = 1; d < 32; d <<= 1) {
+          const long long t = __shfl_up_sync(0xffffffffu, incl, d);
+          if (lane >= d) incl += t;
+        }
+        const long long total = __shfl_sync(0xffffffffu, incl, 31);
+        long long pos = 0;
+        if (lane == 0 && total) pos = (long long)atomicAdd((unsigned long long*)&C->wl_count, (unsigned long long)total);
+        pos = __shfl_sync(0xffffffffu, pos, 0) + (incl - my_nch);
+        for (long long q = 0; q < my_nch && pos + q < A.wl_cap; ++q) A.wl[pos + q] = (my_node << 22) | q;
       }
       for (int t = 0; t < A.kw; ++t)
         if (cnt2[t]) atomicAdd((unsigned long long*)&s_cnt[32 * t + lane], (unsigned long long)cnt2[t]);

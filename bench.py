@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--scale-precisions", default="32,64", help="--scale-run: precisions to run, in order")
     ap.add_argument("--scale-log2n", type=int, default=25,
                     help="the default line's scale block: log2 n of its BA graph (0: no scale block)")
+    ap.add_argument("--scale-maxiter", type=int, default=1000,
+                    help="eigsh_maxiter of the scale solves (the reference's default is 1000)")
     ap.add_argument("--scale-run", action="store_true",
                     help="one timed FP32 solve and one timed plain-FP64 solve of the graph, with the energy gap")
     ap.add_argument("--spmv-layout", choices=["auto", "panel", "split", "worklist"], default="auto",
@@ -536,7 +538,7 @@ def scale_solves(args, dev, n, rowptr, col, val, d_rowptr=None, d_col=None, d_va
         d_val = torch.from_numpy(val).to(dev)
     out = {"n": n, "nnz": nnz, "rowptr": str(d_rowptr.dtype).replace("torch.", ""),
            "workload": f"BA(n={n}, m={args.m}) J=-A, {args.num_alphas} alphas sqrt schedule, diagonal predictor, "
-                       f"eigsh_tol 1e-6, batched local search; CSR resident"}
+                       f"eigsh_tol 1e-6, eigsh_maxiter {args.scale_maxiter}, batched local search; CSR resident"}
     from specann_b200 import graphs as _g
     Jw = _g.barabasi_albert(4096, 8, seed=1)       # load the kernels once (not timed)
     SpectralAnnealing("w.txt", "w", random_seed=1, num_alphas=4, write_results=False).solve(Jw)
@@ -546,7 +548,7 @@ def scale_solves(args, dev, n, rowptr, col, val, d_rowptr=None, d_col=None, d_va
             torch.cuda.empty_cache()
             d_val = torch.from_numpy(val.astype(np.float64)).to(dev)
         s = SpectralAnnealing("scale.txt", "scale", random_seed=42, num_alphas=args.num_alphas, precision=prec,
-                              write_results=False, profile=True)
+                              eigsh_maxiter=args.scale_maxiter, write_results=False, profile=True)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         e, spins, _ = s.solve_device(d_rowptr, d_col, d_val)
@@ -562,6 +564,13 @@ def scale_solves(args, dev, n, rowptr, col, val, d_rowptr=None, d_col=None, d_va
                             "iters_mean": float(np.mean(iters)), "iters_max": int(np.max(iters)),
                             "max_residual": float(np.nanmax(res)),
                             "alphas_above_1e-5": int(sum(1 for x in res if x > 1e-5)),
+                            # alphas that stopped at maxiter unconverged (the reference marks
+                            # them "energy bound not certified" and keeps them)
+                            "uncertified": [{"alpha_index": r["alpha_index"], "alpha": r["alpha"],
+                                             "iterations": r["eigsh_iterations"],
+                                             "residual": r["eigsh_residual"],
+                                             "cold_start": r["alpha_index"] == 0}
+                                            for r in s.alpha_results if not r["eigsh_converged"]],
                             "alphas_skipped": int(s._alphas_skipped),
                             "candidates": int(s._num_candidates or 0),
                             "peak_mem_gb": torch.cuda.max_memory_allocated() / 1e9}

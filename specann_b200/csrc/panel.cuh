@@ -103,6 +103,31 @@ __device__ __forceinline__ void panel_issue(const PanelArgs& P, const T* u, int 
              &bars[buf]);
 }
 
+// Pull `bytes` (a multiple of 16; 16-byte aligned address) of global memory into L2 without a
+// destination in shared memory. One thread; nothing waits for it.
+__device__ __forceinline__ void l2_prefetch_bulk(const void* src, unsigned long long bytes) {
+  constexpr unsigned long long kStep = 1ull << 20;
+  for (unsigned long long o = 0; o < bytes; o += kStep) {
+    const unsigned len = (unsigned)((bytes - o < kStep) ? (bytes - o) : kStep);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"((const char*)src + o), "r"(len) : "memory");
+  }
+}
+
+// Segment (b, q)'s entry words (and values) into L2 ahead of use: the entry stream comes from DRAM,
+// and the one batch that each warp loads ahead does not cover DRAM latency. Segments start on
+// piece boundaries (multiples of kPanelBatchEntries slots), so both streams are 16-byte aligned.
+constexpr int kPanelPrefetch = 2;   // segments prefetched ahead of the panel being processed
+
+template <typename T>
+__device__ __forceinline__ void panel_prefetch(const PanelArgs& P, int b, int q) {
+  if (q >= P.n_panels) return;
+  const long long* ch = P.chunk + ((long long)b * P.n_panels + q) * kWarps;
+  const long long s = __ldg(ch), e = __ldg(ch + kWarps);
+  if (e <= s) return;
+  l2_prefetch_bulk(P.ent + s, (unsigned long long)(e - s) * 4ull);
+  if (P.val) l2_prefetch_bulk((const T*)P.val + s, (unsigned long long)(e - s) * sizeof(T));
+}
+
 // A batch is 256 entries of a warp's chunk: lane l takes the 8 consecutive entries
 // [e + 8 l, e + 8 l + 8) (chunks are padded with kPanelPad words to multiples of 8, so a lane's
 // entries are all real or all padding and its two 16-byte loads are aligned).
@@ -139,22 +164,30 @@ __device__ __forceinline__ void panel_load_vals(const T* val, long long e, long 
   for (int j = 0; j < kPanelLane; ++j) v[j] = (k < ce) ? ld_stream(val + k + j, pol) : T(0);
 }
 
-// Products of one batch added into the block's row sums ys. The entries are in row order, so
+// x with its sign flipped when the sign bit (bit 15) of entry word w is set.
+__device__ __forceinline__ float flip_sign(float x, unsigned w) {
+  return __int_as_float(__float_as_int(x) ^ (int)((w & 0x8000u) << 16));
+}
+__device__ __forceinline__ double flip_sign(double x, unsigned w) {
+  return __longlong_as_double(__double_as_longlong(x) ^ (long long)((unsigned long long)(w & 0x8000u) << 48));
+}
+
+// Products of one batch added into the block's row sums ys. With one coupling magnitude the
+// products are the signed inputs (+-x); the magnitude multiplies the finished row sum. The entries are in row order, so
 // every row is a run of consecutive entries: runs inside a lane are summed in registers (left to
 // right); a run that crosses lanes is summed by a segmented scan over the lanes' tail sums and
 // added by the lane where it ends. Each run is added to ys once per batch, by one lane, and the
 // runs of one lane have distinct rows, so all of a lane's loads of ys can precede its stores.
 template <typename T>
 __device__ __forceinline__ void panel_batch(const unsigned (&r)[kPanelLane], const T (&v)[kPanelLane], bool uniform,
-                                            T wmag, int lane, const T* xs, T* ys) {
+                                            int lane, const T* xs, T* ys) {
   unsigned key[kPanelLane];
   T s[kPanelLane];
 #pragma unroll
   for (int j = 0; j < kPanelLane; ++j) {
     key[j] = r[j] >> 16;
     const T x = xs[r[j] & 0x7FFFu];
-    const T a = uniform ? ((r[j] & 0x8000u) ? -wmag : wmag) : v[j];
-    s[j] = a * x;
+    s[j] = uniform ? flip_sign(x, r[j]) : v[j] * x;
   }
 #pragma unroll
   for (int j = 1; j < kPanelLane; ++j)
@@ -211,6 +244,7 @@ __device__ __forceinline__ bool panel_spmv(const PanelArgs& P, const T* u, int b
     if (threadIdx.x == 0) {
       fence_proxy_async();
       for (int q = 0; q < kPanelBufs && q < np; ++q) panel_issue<T>(P, u, q, smem, bars);
+      for (int q = 0; q <= kPanelPrefetch; ++q) panel_prefetch<T>(P, b, q);
     }
     __syncthreads();
     const long long* ch = P.chunk + (long long)b * np * kWarps + wid;
@@ -250,7 +284,7 @@ __device__ __forceinline__ bool panel_spmv(const PanelArgs& P, const T* u, int b
           panel_load_batch(P.ent, ns, ne, lane, nx, pol);
           if (!uniform) panel_load_vals(val, ns, ne, lane, nv, pol);
         }
-        if (e < ce) panel_batch<T>(cur, cv, uniform, wmag, lane, xs, ys);
+        if (e < ce) panel_batch<T>(cur, cv, uniform, lane, xs, ys);
 #pragma unroll
         for (int q = 0; q < kPanelLane; ++q) {
           cur[q] = nx[q];
@@ -274,12 +308,15 @@ __device__ __forceinline__ bool panel_spmv(const PanelArgs& P, const T* u, int b
         __syncthreads();
         return false;
       }
-      if (threadIdx.x == 0 && p + kPanelBufs < np) {
-        fence_proxy_async();
-        panel_issue<T>(P, u, p + kPanelBufs, smem, bars);
+      if (threadIdx.x == 0) {
+        if (p + kPanelBufs < np) {
+          fence_proxy_async();
+          panel_issue<T>(P, u, p + kPanelBufs, smem, bars);
+        }
+        panel_prefetch<T>(P, b, p + 1 + kPanelPrefetch);
       }
     }
-    for (int i = threadIdx.x; i < nr; i += blockDim.x) fin((long long)r0 + i, ys[i]);
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) fin((long long)r0 + i, uniform ? ys[i] * wmag : ys[i]);
     __syncthreads();
   }
   return true;

@@ -627,101 +627,11 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
 
     // ---------------- Lanczos steps ----------------------------------------------------------
     bool restart_p0 = false;
-    if (pol.block() == 0 && threadIdx.x == 0) {
-      C->gram_ok = 0;
-      C->ritz_ok = 0;
-    }
+    if (pol.block() == 0 && threadIdx.x == 0) C->ritz_ok = 0;
     while (true) {
       const int j = vload(&C->j);
       const int pass2 = vload(&C->pass2);
-      if constexpr (kLayouts) {
-        if (!pass2 && A.use_panel) {
-          // P1 fused (column-panel layout, where every CTA owns whole rows): the SpMV, then on this
-          // CTA's rows the raw dots c_k = V_k . w and the Gram column g_k = V_k . V_j (k <= j) and
-          // |w|^2 in one pass, with no grid barrier in between. The epilogue turns them into the
-          // three-term and Gram-Schmidt coefficients of the step exactly as if the dots had been
-          // taken after the three-term step: h_k = c_k - a g_k - b_{j-1} G_{k, j-1} with a = c_j. One
-          // grid barrier per phase fewer than the separate dot phase, and w is not re-read.
-          const T inv_b = (T)vload(&C->inv_b);
-          T* Vj = A.V + (long long)j * A.ldv;
-          const T trho = (T)rho;
-          if (!apply([&](long long r, T acc) {
-                const T wr = __ldcg(A.w + r);
-                const T vr = wr * inv_b;
-                const T wn = (trho * wr - __ldcg(A.sigma + r) * acc) * inv_b;
-                Vj[r] = vr;
-                A.w[r] = wn;
-              })) return;
-          __syncthreads();
-          const int nbat = (j + kDotBatch) / kDotBatch;
-          double ww = 0.0;
-          for (int kb = 0; kb <= j; kb += kDotBatch) {
-            double cacc[kDotBatch], gacc[kDotBatch];
-#pragma unroll
-            for (int q = 0; q < kDotBatch; ++q) cacc[q] = gacc[q] = 0.0;
-            const int nk = (j + 1 - kb < kDotBatch) ? (j + 1 - kb) : kDotBatch;
-            for (int b = pol.block(); b < A.panel.n_blocks; b += pol.nblocks()) {
-              const long long r0 = __ldg(A.panel.row0 + b), r1 = __ldg(A.panel.row0 + b + 1);
-              for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-                const double wd = (double)__ldcg(A.w + r), vj = (double)__ldcg(Vj + r);
-                if (kb == 0) ww += wd * wd;
-                T vk[kDotBatch];
-#pragma unroll
-                for (int q = 0; q < kDotBatch; ++q)
-                  if (q < nk) vk[q] = __ldcg(A.V + (long long)(kb + q) * A.ldv + r);
-#pragma unroll
-                for (int q = 0; q < kDotBatch; ++q)
-                  if (q < nk) {
-                    cacc[q] += (double)vk[q] * wd;
-                    gacc[q] += (double)vk[q] * vj;
-                  }
-              }
-            }
-            // batch kb: c at columns [2 kb, 2 kb + 8), g at [2 kb + 8, 2 kb + 16)
-            block_store_partials<kDotBatch>(cacc, A.part, A.pw, 2 * kb, sm, pol.block());
-            block_store_partials<kDotBatch>(gacc, A.part, A.pw, 2 * kb + kDotBatch, sm, pol.block());
-          }
-          {
-            double wv[1] = {ww};
-            block_store_partials<1>(wv, A.part, A.pw, 2 * kDotBatch * nbat, sm, pol.block());
-          }
-          if (!pol.sync(&C->gs, [&] {
-                reduce_partials(A.part, A.pw, pol.nblocks(), 2 * kDotBatch * nbat + 1, sm);
-                if (threadIdx.x == 0) {
-                  auto cval = [&](int k) { return sm[2 * ((k / kDotBatch) * kDotBatch) + (k % kDotBatch)]; };
-                  auto gval = [&](int k) { return sm[2 * ((k / kDotBatch) * kDotBatch) + kDotBatch + (k % kDotBatch)]; };
-                  const double a = cval(j);
-                  const double bp = j > 0 ? C->b[j - 1] : 0.0;
-                  const bool gk = C->gram_ok != 0;
-                  // G_{k, j-1} = V_k . V_{j-1}: the previous step's column for k < j, g_{j-1} for k = j
-                  // (symmetry); unit vectors assumed right after a restart (gram_ok = 0)
-                  auto gprev = [&](int k) {
-                    if (k == j) return j > 0 ? gval(j - 1) : 0.0;
-                    return gk ? C->gprev[k] : (k == j - 1 ? 1.0 : 0.0);
-                  };
-                  double hj = 0.0;
-                  for (int k = 0; k <= j; ++k) {
-                    const double hk = cval(k) - a * gval(k) - (j > 0 ? bp * gprev(k) : 0.0);
-                    C->h[k] = hk + (k == j ? a : 0.0) + (k == j - 1 ? bp : 0.0);
-                    if (k == j) hj = hk;
-                  }
-                  // |w - a V_j - b V_{j-1}|^2 (the norm the second-pass test compares with)
-                  const double gjj = gval(j), gjm = j > 0 ? gval(j - 1) : 0.0, gmm = j > 0 ? gprev(j - 1) : 0.0;
-                  const double cjm = j > 0 ? cval(j - 1) : 0.0;
-                  C->ww = sm[2 * kDotBatch * nbat] - 2.0 * a * a - 2.0 * bp * cjm + a * a * gjj + 2.0 * a * bp * gjm +
-                          bp * bp * gmm;
-                  C->a[j] = a + hj;
-                  for (int k = 0; k <= j; ++k) C->gprev[k] = gval(k);
-                  C->gram_ok = 1;
-                  C->bytes += A.spmv_bytes + (double)n * sizeof(T) * (double)(j + 3);
-                  C->spmvs += 1;
-                }
-              })) return;
-          mark(1);
-        }
-      }
-      const bool fused = kLayouts && A.use_panel && !pass2;
-      if (!pass2 && !fused) {
+      if (!pass2) {
         // P1: V[j] = w * inv_b; w <- S V[j]; partial sums of a_j = V[j] . w
         const T inv_b = (T)vload(&C->inv_b);
         T* Vj = A.V + (long long)j * A.ldv;
@@ -748,9 +658,8 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
       }
       // P2: three-term step w -= a_j V[j] + b_{j-1} V[j-1] (first pass only), then the
       // reorthogonalisation coefficients h_k = V_k . w (k <= j) and ww = w . w. Removing the
-      // dominant components explicitly first keeps the single Gram-Schmidt pass stable. (The fused
-      // first pass of the panel layout has its coefficients from the P1 epilogue already.)
-      if (!fused) {
+      // dominant components explicitly first keeps the single Gram-Schmidt pass stable.
+      {
         const double a3 = pass2 ? 0.0 : vload(&C->a[j]);
         const double b3 = (pass2 || j == 0) ? 0.0 : vload(&C->b[j - 1]);
         const T* Vj = A.V + (long long)j * A.ldv;
@@ -936,7 +845,6 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
                   C->action = ACT_DONE;
                 } else if (m >= ncv) {
                   C->restarts += 1;
-                  C->gram_ok = 0;          // the kept basis is rotated: its Gram column is not known
                   C->action = ACT_RESTART;
                 } else {
                   C->b[j] = bj;

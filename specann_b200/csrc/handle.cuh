@@ -45,8 +45,6 @@ struct AlphaCtrl {
   double irl_beta;          // T+[k][k-1] of the last implicit restart
   double irl_sigma;         // Q[m-1][k-1] of the last implicit restart
   unsigned long long tph[6];  // ns by phase (set-up, SpMV, dots, update+Ritz, restart, final)
-  double gprev[kNcvMax];    // Gram column V_k . V_{j-1} of the previous step (fused first pass)
-  int gram_ok;              // gprev holds that column (0 at the start and after a restart)
   int ritz_ok;              // theta / res_est hold the previous step's Ritz value and residual estimate
 };
 

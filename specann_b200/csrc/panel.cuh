@@ -118,11 +118,17 @@ __device__ __forceinline__ void l2_prefetch_bulk(const void* src, unsigned long 
 // piece boundaries (multiples of kPanelBatchEntries slots), so both streams are 16-byte aligned.
 constexpr int kPanelPrefetch = 2;   // segments prefetched ahead of the panel being processed
 
-template <typename T>
-__device__ __forceinline__ void panel_prefetch(const PanelArgs& P, int b, int q) {
+// Slots [s, e) of segment (b, q); empty when q is past the last panel.
+__device__ __forceinline__ void panel_segment(const PanelArgs& P, int b, int q, long long& s, long long& e) {
+  s = e = 0;
   if (q >= P.n_panels) return;
   const long long* ch = P.chunk + ((long long)b * P.n_panels + q) * kWarps;
-  const long long s = __ldg(ch), e = __ldg(ch + kWarps);
+  s = __ldg(ch);
+  e = __ldg(ch + kWarps);
+}
+
+template <typename T>
+__device__ __forceinline__ void panel_prefetch(const PanelArgs& P, long long s, long long e) {
   if (e <= s) return;
   l2_prefetch_bulk(P.ent + s, (unsigned long long)(e - s) * 4ull);
   if (P.val) l2_prefetch_bulk((const T*)P.val + s, (unsigned long long)(e - s) * sizeof(T));
@@ -164,30 +170,22 @@ __device__ __forceinline__ void panel_load_vals(const T* val, long long e, long 
   for (int j = 0; j < kPanelLane; ++j) v[j] = (k < ce) ? ld_stream(val + k + j, pol) : T(0);
 }
 
-// x with its sign flipped when the sign bit (bit 15) of entry word w is set.
-__device__ __forceinline__ float flip_sign(float x, unsigned w) {
-  return __int_as_float(__float_as_int(x) ^ (int)((w & 0x8000u) << 16));
-}
-__device__ __forceinline__ double flip_sign(double x, unsigned w) {
-  return __longlong_as_double(__double_as_longlong(x) ^ (long long)((unsigned long long)(w & 0x8000u) << 48));
-}
-
-// Products of one batch added into the block's row sums ys. With one coupling magnitude the
-// products are the signed inputs (+-x); the magnitude multiplies the finished row sum. The entries are in row order, so
+// Products of one batch added into the block's row sums ys. The entries are in row order, so
 // every row is a run of consecutive entries: runs inside a lane are summed in registers (left to
 // right); a run that crosses lanes is summed by a segmented scan over the lanes' tail sums and
 // added by the lane where it ends. Each run is added to ys once per batch, by one lane, and the
 // runs of one lane have distinct rows, so all of a lane's loads of ys can precede its stores.
 template <typename T>
 __device__ __forceinline__ void panel_batch(const unsigned (&r)[kPanelLane], const T (&v)[kPanelLane], bool uniform,
-                                            int lane, const T* xs, T* ys) {
+                                            T wmag, int lane, const T* xs, T* ys) {
   unsigned key[kPanelLane];
   T s[kPanelLane];
 #pragma unroll
   for (int j = 0; j < kPanelLane; ++j) {
     key[j] = r[j] >> 16;
     const T x = xs[r[j] & 0x7FFFu];
-    s[j] = uniform ? flip_sign(x, r[j]) : v[j] * x;
+    const T a = uniform ? ((r[j] & 0x8000u) ? -wmag : wmag) : v[j];
+    s[j] = a * x;
   }
 #pragma unroll
   for (int j = 1; j < kPanelLane; ++j)
@@ -244,7 +242,11 @@ __device__ __forceinline__ bool panel_spmv(const PanelArgs& P, const T* u, int b
     if (threadIdx.x == 0) {
       fence_proxy_async();
       for (int q = 0; q < kPanelBufs && q < np; ++q) panel_issue<T>(P, u, q, smem, bars);
-      for (int q = 0; q <= kPanelPrefetch; ++q) panel_prefetch<T>(P, b, q);
+      for (int q = 0; q <= kPanelPrefetch; ++q) {
+        long long s0, e0;
+        panel_segment(P, b, q, s0, e0);
+        panel_prefetch<T>(P, s0, e0);
+      }
     }
     __syncthreads();
     const long long* ch = P.chunk + (long long)b * np * kWarps + wid;
@@ -254,8 +256,11 @@ __device__ __forceinline__ bool panel_spmv(const PanelArgs& P, const T* u, int b
     panel_load_batch(P.ent, cs, ce, lane, cur, pol);
     if (!uniform) panel_load_vals(val, cs, ce, lane, cv, pol);
     for (int p = 0; p < np; ++p) {
-      // the next panel's chunk bounds, consumed at the end of this panel
-      long long ns = 0, ne = 0;
+      // the next panel's chunk bounds, and (thread 0) the bounds of the segment to prefetch at the
+      // end of this panel: both consumed at the end of this panel, so their loads are in flight
+      // while the panel is processed
+      long long ns = 0, ne = 0, pfs = 0, pfe = 0;
+      if (threadIdx.x == 0) panel_segment(P, b, p + 1 + kPanelPrefetch, pfs, pfe);
       if (p + 1 < np) {
         ns = __ldg(ch + (long long)(p + 1) * kWarps);
         ne = __ldg(ch + (long long)(p + 1) * kWarps + 1);
@@ -284,7 +289,7 @@ __device__ __forceinline__ bool panel_spmv(const PanelArgs& P, const T* u, int b
           panel_load_batch(P.ent, ns, ne, lane, nx, pol);
           if (!uniform) panel_load_vals(val, ns, ne, lane, nv, pol);
         }
-        if (e < ce) panel_batch<T>(cur, cv, uniform, lane, xs, ys);
+        if (e < ce) panel_batch<T>(cur, cv, uniform, wmag, lane, xs, ys);
 #pragma unroll
         for (int q = 0; q < kPanelLane; ++q) {
           cur[q] = nx[q];
@@ -313,10 +318,10 @@ __device__ __forceinline__ bool panel_spmv(const PanelArgs& P, const T* u, int b
           fence_proxy_async();
           panel_issue<T>(P, u, p + kPanelBufs, smem, bars);
         }
-        panel_prefetch<T>(P, b, p + 1 + kPanelPrefetch);
+        panel_prefetch<T>(P, pfs, pfe);
       }
     }
-    for (int i = threadIdx.x; i < nr; i += blockDim.x) fin((long long)r0 + i, uniform ? ys[i] * wmag : ys[i]);
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) fin((long long)r0 + i, ys[i]);
     __syncthreads();
   }
   return true;

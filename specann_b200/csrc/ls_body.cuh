@@ -240,7 +240,6 @@ __device__ __forceinline__ void ls_body(const LsArgs<VT, RP, GT>& A, const Pol& 
         if (A.priority) A.prio[tile + lane] = selb ? rk : 0x7fffffff;
       }
       const uint32_t selmask = __ballot_sync(0xffffffffu, selb);
-      uint32_t tile_want = 0u;   // priority passes: bit l set if node tile + l wants to flip
       for (int sub = 0; sub < 32; sub += ne) {
         const long long i = tile + sub + slot;
         const bool valid = i < n && ((selmask >> (sub + slot)) & 1u);
@@ -267,6 +266,10 @@ __device__ __forceinline__ void ls_body(const LsArgs<VT, RP, GT>& A, const Pol& 
           for (int t = 0; t < A.kw; ++t) any |= fl[t];
           if (A.priority) {
             for (int t = 0; t < A.kw; ++t) A.wm[i * A.kw + t] = fl[t];
+            if (any) {
+              const long long pos = (long long)atomicAdd((unsigned long long*)&C->wq_count, 1ull);
+              A.wq[pos] = (int)i;
+            }
           } else if (any) {
             for (int t = 0; t < A.kw; ++t) A.flipm[i * A.kw + t] = fl[t];
             const long long deg = rp_load(A.rowptr, i + 1) - rp_load(A.rowptr, i);
@@ -275,21 +278,6 @@ __device__ __forceinline__ void ls_body(const LsArgs<VT, RP, GT>& A, const Pol& 
             for (long long q = 0; q < nch && pos + q < A.wl_cap; ++q) A.wl[pos + q] = (i << 22) | q;
           }
         }
-        if (A.priority) {
-          // the wanting nodes of this sub-step (one lane per node slot holds `any`)
-          uint32_t anyw = 0u;
-          for (int t = 0; t < A.kw; ++t) anyw |= fl[t];
-          const uint32_t wb = __ballot_sync(0xffffffffu, c == 0 && i < n && anyw != 0u);
-          for (int sl = 0; sl < ne; ++sl)
-            if ((wb >> (sl * cp)) & 1u) tile_want |= 1u << (sub + sl);
-        }
-      }
-      if (A.priority && tile_want) {
-        // one queue reservation per tile of 32 nodes (in node order within the tile)
-        long long pos = 0;
-        if (lane == 0) pos = (long long)atomicAdd((unsigned long long*)&C->wq_count, (unsigned long long)__popc(tile_want));
-        pos = __shfl_sync(0xffffffffu, pos, 0);
-        if ((tile_want >> lane) & 1u) A.wq[pos + __popc(tile_want & ((1u << lane) - 1u))] = (int)(tile + lane);
       }
     }
     if (!A.priority) {
@@ -301,54 +289,37 @@ __device__ __forceinline__ void ls_body(const LsArgs<VT, RP, GT>& A, const Pol& 
     } else {
       if (!pol.sync(&C->gs)) return;
       // D2: a wanting node flips the candidates for which no wanting neighbour has a lower rank
-      // (one warp per wanting node, 32 consecutive queue entries per warp; the blocking masks are
-      // OR-reduced over the row; the flipping nodes' work-list chunks are reserved with one atomic
-      // per 32 nodes)
+      // (one warp per wanting node; the blocking masks are OR-reduced over the row)
       const long long nwq = *((volatile long long*)&C->wq_count);
       int cnt2[4] = {0, 0, 0, 0};
-      for (long long base = gwarp * 32; base < nwq; base += nwarps * 32) {
-        long long my_node = 0, my_nch = 0;   // lane q: node base + q and its chunks if it flips
-        for (int q = 0; q < 32 && base + q < nwq; ++q) {
-          const long long i = (long long)__ldcg(A.wq + base + q);
-          const int pi = __ldcg(A.prio + i);
-          uint32_t W[4] = {0u, 0u, 0u, 0u}, B[4] = {0u, 0u, 0u, 0u};
-          for (int t = 0; t < A.kw; ++t) W[t] = __ldcg(A.wm + i * A.kw + t);
-          const long long rs = rp_load(A.rowptr, i), re = rp_load(A.rowptr, i + 1);
-          for (long long p = rs + lane; p < re; p += 32) {
-            const int j = __ldg(A.col + p);
-            if (__ldcg(A.prio + j) < pi)
-              for (int t = 0; t < A.kw; ++t) B[t] |= __ldcg(A.wm + (long long)j * A.kw + t);
-          }
-          uint32_t any = 0u;
+      for (long long e = gwarp; e < nwq; e += nwarps) {
+        const long long i = (long long)__ldcg(A.wq + e);
+        const int pi = __ldcg(A.prio + i);
+        uint32_t W[4] = {0u, 0u, 0u, 0u}, B[4] = {0u, 0u, 0u, 0u};
+        for (int t = 0; t < A.kw; ++t) W[t] = __ldcg(A.wm + i * A.kw + t);
+        const long long rs = rp_load(A.rowptr, i), re = rp_load(A.rowptr, i + 1);
+        for (long long p = rs + lane; p < re; p += 32) {
+          const int j = __ldg(A.col + p);
+          if (__ldcg(A.prio + j) < pi)
+            for (int t = 0; t < A.kw; ++t) B[t] |= __ldcg(A.wm + (long long)j * A.kw + t);
+        }
+        uint32_t any = 0u;
+        for (int t = 0; t < A.kw; ++t) {
+          B[t] = __reduce_or_sync(0xffffffffu, B[t]);
+          W[t] &= ~B[t];
+          any |= W[t];
+          cnt2[t] += (W[t] >> lane) & 1u;
+        }
+        if (lane == 0 && any) {
           for (int t = 0; t < A.kw; ++t) {
-            B[t] = __reduce_or_sync(0xffffffffu, B[t]);
-            W[t] &= ~B[t];
-            any |= W[t];
-            cnt2[t] += (W[t] >> lane) & 1u;
+            A.flipm[i * A.kw + t] = W[t];
+            if (W[t]) A.sb[i * A.kw + t] = __ldcg(A.sb + i * A.kw + t) ^ W[t];
           }
-          if (lane == 0 && any) {
-            for (int t = 0; t < A.kw; ++t) {
-              A.flipm[i * A.kw + t] = W[t];
-              if (W[t]) A.sb[i * A.kw + t] = __ldcg(A.sb + i * A.kw + t) ^ W[t];
-            }
-          }
-          if (lane == q) {
-            my_node = i;
-            const long long deg = re - rs;
-            my_nch = any ? (deg > kChunk ? (deg + kChunk - 1) / kChunk : 1) : 0;
-          }
+          const long long deg = re - rs;
+          const long long nch = deg > kChunk ? (deg + kChunk - 1) / kChunk : 1;
+          const long long pos = (long long)atomicAdd((unsigned long long*)&C->wl_count, (unsigned long long)nch);
+          for (long long q = 0; q < nch && pos + q < A.wl_cap; ++q) A.wl[pos + q] = (i << 22) | q;
         }
-        // exclusive scan of the chunk counts over the lanes, one reservation for the warp
-        long long incl = my_nch;
-        for (int d = 1; d < 32; d <<= 1) {
-          const long long t = __shfl_up_sync(0xffffffffu, incl, d);
-          if (lane >= d) incl += t;
-        }
-        const long long total = __shfl_sync(0xffffffffu, incl, 31);
-        long long pos = 0;
-        if (lane == 0 && total) pos = (long long)atomicAdd((unsigned long long*)&C->wl_count, (unsigned long long)total);
-        pos = __shfl_sync(0xffffffffu, pos, 0) + (incl - my_nch);
-        for (long long q = 0; q < my_nch && pos + q < A.wl_cap; ++q) A.wl[pos + q] = (my_node << 22) | q;
       }
       for (int t = 0; t < A.kw; ++t)
         if (cnt2[t]) atomicAdd((unsigned long long*)&s_cnt[32 * t + lane], (unsigned long long)cnt2[t]);

@@ -103,37 +103,6 @@ __device__ __forceinline__ void panel_issue(const PanelArgs& P, const T* u, int 
              &bars[buf]);
 }
 
-// Pull `bytes` (a multiple of 16; 16-byte aligned address) of global memory into L2 without a
-// destination in shared memory. One thread; nothing waits for it.
-__device__ __forceinline__ void l2_prefetch_bulk(const void* src, unsigned long long bytes) {
-  constexpr unsigned long long kStep = 1ull << 20;
-  for (unsigned long long o = 0; o < bytes; o += kStep) {
-    const unsigned len = (unsigned)((bytes - o < kStep) ? (bytes - o) : kStep);
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"((const char*)src + o), "r"(len) : "memory");
-  }
-}
-
-// Segment (b, q)'s entry words (and values) into L2 ahead of use: the entry stream comes from DRAM,
-// and the one batch that each warp loads ahead does not cover DRAM latency. Segments start on
-// piece boundaries (multiples of kPanelBatchEntries slots), so both streams are 16-byte aligned.
-constexpr int kPanelPrefetch = 2;   // segments prefetched ahead of the panel being processed
-
-// Slots [s, e) of segment (b, q); empty when q is past the last panel.
-__device__ __forceinline__ void panel_segment(const PanelArgs& P, int b, int q, long long& s, long long& e) {
-  s = e = 0;
-  if (q >= P.n_panels) return;
-  const long long* ch = P.chunk + ((long long)b * P.n_panels + q) * kWarps;
-  s = __ldg(ch);
-  e = __ldg(ch + kWarps);
-}
-
-template <typename T>
-__device__ __forceinline__ void panel_prefetch(const PanelArgs& P, long long s, long long e) {
-  if (e <= s) return;
-  l2_prefetch_bulk(P.ent + s, (unsigned long long)(e - s) * 4ull);
-  if (P.val) l2_prefetch_bulk((const T*)P.val + s, (unsigned long long)(e - s) * sizeof(T));
-}
-
 // A batch is 256 entries of a warp's chunk: lane l takes the 8 consecutive entries
 // [e + 8 l, e + 8 l + 8) (chunks are padded with kPanelPad words to multiples of 8, so a lane's
 // entries are all real or all padding and its two 16-byte loads are aligned).
@@ -242,11 +211,6 @@ __device__ __forceinline__ bool panel_spmv(const PanelArgs& P, const T* u, int b
     if (threadIdx.x == 0) {
       fence_proxy_async();
       for (int q = 0; q < kPanelBufs && q < np; ++q) panel_issue<T>(P, u, q, smem, bars);
-      for (int q = 0; q <= kPanelPrefetch; ++q) {
-        long long s0, e0;
-        panel_segment(P, b, q, s0, e0);
-        panel_prefetch<T>(P, s0, e0);
-      }
     }
     __syncthreads();
     const long long* ch = P.chunk + (long long)b * np * kWarps + wid;
@@ -256,11 +220,8 @@ __device__ __forceinline__ bool panel_spmv(const PanelArgs& P, const T* u, int b
     panel_load_batch(P.ent, cs, ce, lane, cur, pol);
     if (!uniform) panel_load_vals(val, cs, ce, lane, cv, pol);
     for (int p = 0; p < np; ++p) {
-      // the next panel's chunk bounds, and (thread 0) the bounds of the segment to prefetch at the
-      // end of this panel: both consumed at the end of this panel, so their loads are in flight
-      // while the panel is processed
-      long long ns = 0, ne = 0, pfs = 0, pfe = 0;
-      if (threadIdx.x == 0) panel_segment(P, b, p + 1 + kPanelPrefetch, pfs, pfe);
+      // the next panel's chunk bounds, consumed at the end of this panel
+      long long ns = 0, ne = 0;
       if (p + 1 < np) {
         ns = __ldg(ch + (long long)(p + 1) * kWarps);
         ne = __ldg(ch + (long long)(p + 1) * kWarps + 1);
@@ -313,12 +274,9 @@ __device__ __forceinline__ bool panel_spmv(const PanelArgs& P, const T* u, int b
         __syncthreads();
         return false;
       }
-      if (threadIdx.x == 0) {
-        if (p + kPanelBufs < np) {
-          fence_proxy_async();
-          panel_issue<T>(P, u, p + kPanelBufs, smem, bars);
-        }
-        panel_prefetch<T>(P, pfs, pfe);
+      if (threadIdx.x == 0 && p + kPanelBufs < np) {
+        fence_proxy_async();
+        panel_issue<T>(P, u, p + kPanelBufs, smem, bars);
       }
     }
     for (int i = threadIdx.x; i < nr; i += blockDim.x) fin((long long)r0 + i, ys[i]);

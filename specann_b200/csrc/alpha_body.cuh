@@ -743,37 +743,59 @@ __device__ __forceinline__ void alpha_body(const AlphaArgs<T, RP>& A, const Pol&
         double v[1] = {0.0};
         constexpr int VW = 16 / sizeof(T);
         const long long nvec = n / VW;
-        for (long long iv = gtid; iv < nvec; iv += nthreads) {
-          const long long i0 = iv * VW;
+        // U positions per thread and iteration (iv, iv + nthreads), whose loads are in flight
+        // together, and KB3 basis vectors per batch (the same registers as one position and
+        // kDotBatch vectors); the batch kernel keeps one position within its register budget
+        constexpr int U = kLayouts ? 2 : 1;
+        constexpr int KB3 = kDotBatch / U;
+        for (long long iv = gtid; iv < nvec; iv += U * nthreads) {
+          const bool two = U == 2 && iv + nthreads < nvec;
+          const long long i0[2] = {iv * VW, (two ? iv + nthreads : iv) * VW};
           // w and sigma are put in flight first; the basis is read kDotBatch vectors at a time
-          T wv[VW], sg[VW], uv[VW];
-          ld16(A.w + i0, wv);
-          ld16(A.sigma + i0, sg);
-          double corr[VW];
+          T wv[2][VW], sg[2][VW];
 #pragma unroll
-          for (int r = 0; r < VW; ++r) corr[r] = 0.0;
-          for (int kb = 0; kb <= j; kb += kDotBatch) {
-            T vk[kDotBatch][VW];
+          for (int u = 0; u < U; ++u) {
+            ld16(A.w + i0[u], wv[u]);
+            ld16(A.sigma + i0[u], sg[u]);
+          }
+          double corr[2][VW];
 #pragma unroll
-            for (int q = 0; q < kDotBatch; ++q) {
-              if (kb + q <= j) ld16(A.V + (long long)(kb + q) * A.ldv + i0, vk[q]);
-            }
+          for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int q = 0; q < kDotBatch; ++q) {
+            for (int r = 0; r < VW; ++r) corr[u][r] = 0.0;
+          for (int kb = 0; kb <= j; kb += KB3) {
+            T vk[KB3][2][VW];
+#pragma unroll
+            for (int q = 0; q < KB3; ++q) {
               if (kb + q <= j) {
 #pragma unroll
-                for (int r = 0; r < VW; ++r) corr[r] += sh[kb + q] * (double)vk[q][r];
+                for (int u = 0; u < U; ++u) ld16(A.V + (long long)(kb + q) * A.ldv + i0[u], vk[q][u]);
+              }
+            }
+#pragma unroll
+            for (int q = 0; q < KB3; ++q) {
+              if (kb + q <= j) {
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                  for (int r = 0; r < VW; ++r) corr[u][r] += sh[kb + q] * (double)vk[q][u][r];
               }
             }
           }
 #pragma unroll
-          for (int r = 0; r < VW; ++r) {
-            wv[r] = (T)((double)wv[r] - corr[r]);
-            uv[r] = sg[r] * wv[r];
-            v[0] += (double)wv[r] * (double)wv[r];
+          for (int u = 0; u < U; ++u) {
+            T uv[VW];
+#pragma unroll
+            for (int r = 0; r < VW; ++r) {
+              wv[u][r] = (T)((double)wv[u][r] - corr[u][r]);
+              uv[r] = sg[u][r] * wv[u][r];
+              if (u == 0 || two) v[0] += (double)wv[u][r] * (double)wv[u][r];
+            }
+            if (u == 0 || two) {
+              st16(A.w + i0[u], wv[u]);
+              st16(A.u + i0[u], uv);
+            }
           }
-          st16(A.w + i0, wv);
-          st16(A.u + i0, uv);
         }
         for (long long i = nvec * VW + gtid; i < n; i += nthreads) {
           const double corr = basis_combine(A.V, A.ldv, i, j, sh);

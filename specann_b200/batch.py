@@ -127,7 +127,7 @@ class BatchedSpectralAnnealing:
             if J.nnz >= 2 ** 31:
                 raise ValueError("batched instances need fewer than 2^31 stored entries")
             eng = Engine(J.shape[0], J.nnz, precision=self.precision, ncv_max=2, max_candidates=1)
-            data = J.data.astype(np.float32 if self.precision == 32 else np.float64)
+            data = J.data.astype(np.float32 if self.precision == 32 else np.float64, copy=False)
             eng.upload_csr(J.indptr, J.indices, data)
             self.engines.append(eng)
         return self
